@@ -1,0 +1,241 @@
+/*
+ * vsmc_cuda.h -- C ABI of libvsmc_cuda, the B200 (sm_100a) SMC step.
+ *
+ * Plain pointers, sizes and status codes only.  Every entry point names the
+ * vSMC interface it replaces (paths relative to the vSMC project root).
+ * Device pointers are CUDA global-memory addresses on the current device;
+ * `stream` is a cudaStream_t (NULL = legacy default stream).
+ *
+ * Errors: every function returns VSMC_CUDA_OK (0) or one of the codes below;
+ * vsmc_cuda_last_error() gives the calling thread's last message.  This
+ * replaces VSMC_RUNTIME_ASSERT (include/vsmc/internal/assert.hpp:60-99);
+ * the C++ facade (include/vsmc_b200/vsmc.hpp) turns codes into exceptions.
+ */
+#ifndef VSMC_CUDA_H
+#define VSMC_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VSMC_CUDA_ABI_VERSION 1
+
+enum vsmc_cuda_status {
+    VSMC_CUDA_OK = 0,
+    VSMC_CUDA_EINVAL = 1,      /* bad argument (size, scheme, null pointer) */
+    VSMC_CUDA_ENOMEM = 2,      /* device allocation or HBM budget exceeded */
+    VSMC_CUDA_EDEGENERATE = 3, /* all log-weights -inf, or NaN/inf weights */
+    VSMC_CUDA_ETIMEOUT = 4,    /* a bounded device-side wait gave up */
+    VSMC_CUDA_ECUDA = 5        /* CUDA runtime error (message has details) */
+};
+
+/* Same values as vsmc::ResampleScheme (include/vsmc/resample/common.hpp:
+ * 124-131). */
+enum vsmc_cuda_scheme {
+    VSMC_CUDA_MULTINOMIAL = 0,
+    VSMC_CUDA_RESIDUAL = 1,
+    VSMC_CUDA_STRATIFIED = 2,
+    VSMC_CUDA_SYSTEMATIC = 3,
+    VSMC_CUDA_RESIDUAL_STRATIFIED = 4,
+    VSMC_CUDA_RESIDUAL_SYSTEMATIC = 5
+};
+
+/* Precision forms of the particle move. */
+enum vsmc_cuda_form {
+    VSMC_CUDA_FP64 = 0, /* everything in double (the reference's layout) */
+    VSMC_CUDA_MIXED = 1 /* float state, move and log-weights; double
+                           cumulative-weight scan and log-evidence */
+};
+
+const char *vsmc_cuda_status_string(int status);
+const char *vsmc_cuda_last_error(void);
+int vsmc_cuda_abi_version(void);
+
+/* ------------------------------------------------------------- RNG ------ */
+
+/* n successive outputs of PhiloxEngine<uint32_t,4,10>::operator()() after
+ * key(key), ctr(ctr) and `skip` discarded draws, written to device `out`.
+ * Replaces include/vsmc/rng/philox.hpp:367-395 (ctr/key/operator()). */
+int vsmc_cuda_philox4x32_words(const uint32_t key[2], const uint32_t ctr[4],
+                               uint64_t skip, uint64_t n, uint32_t *out,
+                               void *stream);
+
+/* Same for ThreefryEngine<uint64_t,4,20> (include/vsmc/rng/threefry.hpp:
+ * 336-364). */
+int vsmc_cuda_threefry4x64_words(const uint64_t key[4], const uint64_t ctr[4],
+                                 uint64_t skip, uint64_t n, uint64_t *out,
+                                 void *stream);
+
+/* Position of a Threefry4x64 resample engine: the next word drawn is lane
+ * (offset % 4) of block ctr + offset / 4 + 1.  A freshly seeded engine
+ * (Threefry4x64(s)) is {key = {s,0,0,0}, ctr = 0, offset = 0}. */
+typedef struct {
+    uint64_t key[4];
+    uint64_t ctr[4];
+    uint64_t offset;
+} vsmc_cuda_threefry_state;
+
+/* ------------------------------------------------------------ weights --- */
+
+/* WeightSet::set_log_weight (inc == NULL) or add_log_weight(inc) on device
+ * arrays: log_weight += inc; log_weight -= max; weight = exp(log_weight) /
+ * sum; *ess = 1 / sum(weight^2).  log_weight is updated in place (max-
+ * normalised, as the reference stores it); weight may be NULL.  Blocks until
+ * *ess is known.  Replaces include/vsmc/core/weight_set.hpp:297-331 and
+ * post_set_log_weight :441-446. */
+int vsmc_cuda_weight_add_log(uint64_t N, double *log_weight, double *weight,
+                             const double *inc, double *ess, void *stream);
+
+/* ----------------------------------------------------------- resample --- */
+
+/* Bytes of device workspace vsmc_cuda_resample needs for N particles. */
+size_t vsmc_cuda_resample_workspace_size(uint64_t N);
+
+/* Resample<Scheme>::operator()(N, N, rng, weight, replication) followed by
+ * internal::cfrp_trans(N, N, replication, copy_from) (include/vsmc/resample/
+ * *.hpp, common.hpp:57-118; Particle::resample, core/particle.hpp:230-250).
+ *
+ * weight: N normalised weights (device).  replication, copy_from: N int32
+ * (device; copy_from may be NULL).  rng: the resample engine position; on
+ * return it has advanced by exactly the words the reference would draw.
+ * uniforms: NULL to draw the U01 sequence from rng on the device (bit-exact
+ * words; the Multinomial sequence goes through log/exp and so matches to a
+ * few ulps), or a device array of the sequence values u_0..u_{k-1} that the
+ * reference's inversion would query (parity mode; k = n_uniforms, entries
+ * beyond k are taken as +inf).  Blocks until the engine position is known.
+ */
+int vsmc_cuda_resample(int scheme, uint64_t N, const double *weight,
+                       const double *uniforms, uint64_t n_uniforms,
+                       vsmc_cuda_threefry_state *rng, int32_t *replication,
+                       int32_t *copy_from, void *workspace,
+                       size_t workspace_bytes, void *stream);
+
+/* StateMatrix<ColMajor, dim, double>::copy(N, copy_from)
+ * (include/vsmc/core/state_matrix.hpp:378-394): dst[d*N + i] =
+ * src[d*N + copy_from[i]] for every column d (src != dst). */
+int vsmc_cuda_copy_f64(uint64_t N, uint32_t dim, const double *src,
+                       double *dst, const int32_t *copy_from, void *stream);
+
+/* ------------------------------------------------ CV Student-t filter ---- */
+
+/* The constant-velocity Student-t bootstrap filter of example/pf
+ * (include/pf_smp.hpp:73-258) as one device-resident object: Sampler<T>
+ * with a StateMatrix<ColMajor,4> value, a Philox4x32 per-particle stream
+ * (counter {block, step, id, stream_id}, key {seed+1, 0}) and the default
+ * Threefry4x64 resample engine seeded seed+2 (Seed::set(seed) semantics,
+ * include/vsmc/rng/seed.hpp:102,149; core/particle.hpp:64-70). */
+typedef struct vsmc_cuda_cv_filter vsmc_cuda_cv_filter;
+
+typedef struct {
+    uint64_t N;          /* particles */
+    uint64_t T_max;      /* capacity of the observation / history arrays */
+    int scheme;          /* vsmc_cuda_scheme */
+    int form;            /* vsmc_cuda_form */
+    double threshold;    /* resample when ESS < threshold * N */
+    uint32_t seed;       /* Seed::set(seed) */
+    uint32_t stream_id;  /* 4th counter word, distinguishes filters */
+    double dt, sd_pos, sd_vel, sd_pos0, sd_vel0, scale, nu;
+} vsmc_cuda_cv_config;
+
+/* N = 0, T_max = 0, Multinomial, FP64, threshold 0.5, seed 101, stream 0,
+ * dt 0.1, sd_pos 0.02, sd_vel 0.5, sd_pos0 2, sd_vel0 1, scale 10, nu 10. */
+void vsmc_cuda_cv_config_default(vsmc_cuda_cv_config *cfg);
+
+/* Device bytes a filter with this configuration allocates. */
+size_t vsmc_cuda_cv_device_bytes(const vsmc_cuda_cv_config *cfg);
+
+/* Sampler<T>(N, scheme, threshold) (core/sampler.hpp:80-104).  All device
+ * memory is allocated here; later calls allocate nothing. */
+int vsmc_cuda_cv_create(const vsmc_cuda_cv_config *cfg, void *stream,
+                        vsmc_cuda_cv_filter **out);
+int vsmc_cuda_cv_destroy(vsmc_cuda_cv_filter *f);
+
+/* Observations y_0..y_{T-1} (x and y coordinates), host or device memory
+ * (cv_state::read_data, pf_smp.hpp:114-125).  Host arrays are copied
+ * asynchronously on the filter's stream (pinned memory recommended). */
+int vsmc_cuda_cv_set_observations(vsmc_cuda_cv_filter *f, const double *obs_x,
+                                  const double *obs_y, uint64_t T,
+                                  int on_device);
+
+/* Sampler::initialize (core/sampler.hpp:450-463): reset histories, draw the
+ * prior, weight by y_0, possibly resample.  Asynchronous. */
+int vsmc_cuda_cv_initialize(vsmc_cuda_cv_filter *f);
+
+/* Sampler::iterate(num) (core/sampler.hpp:471-483): num steps of move,
+ * weight update, ESS test and resampling, monitor.  Asynchronous. */
+int vsmc_cuda_cv_iterate(vsmc_cuda_cv_filter *f, uint64_t num);
+
+/* Waits for the filter's stream and reports sticky device-side errors
+ * (VSMC_CUDA_EDEGENERATE, VSMC_CUDA_ETIMEOUT). */
+int vsmc_cuda_cv_synchronize(vsmc_cuda_cv_filter *f);
+
+/* Number of completed steps (Sampler::iter_size). */
+int vsmc_cuda_cv_iter_size(vsmc_cuda_cv_filter *f, uint64_t *iter_size);
+
+/* Histories (host arrays of iter_size entries, each may be NULL):
+ * Sampler::ess_history / resampled_history (core/sampler.hpp:293-307), the
+ * per-step log-evidence increments (example/include/move_smc.hpp:63-71) and
+ * the MonitorMCMC-stage importance-sampling estimates of the position
+ * (Monitor::record, core/monitor.hpp:181-217).  Synchronises. */
+int vsmc_cuda_cv_history(vsmc_cuda_cv_filter *f, double *ess,
+                         int32_t *resampled, double *logz_inc, double *mean_x,
+                         double *mean_y);
+
+/* Running log-evidence sum (host scalar).  Synchronises. */
+int vsmc_cuda_cv_log_evidence(vsmc_cuda_cv_filter *f, double *logz);
+
+/* Current particles in double, SoA host arrays of N (each may be NULL), and
+ * the max-normalised log-weights (WeightSet::read_log_weight,
+ * core/weight_set.hpp:199-211).  Synchronises. */
+int vsmc_cuda_cv_read_state(vsmc_cuda_cv_filter *f, double *x, double *y,
+                            double *vx, double *vy, double *log_weight);
+
+/* Appends n observations after the ones already set (streaming use: one
+ * per step as it arrives).  Host arrays are copied asynchronously on the
+ * filter's stream and must stay valid until the stream reaches the copy. */
+int vsmc_cuda_cv_append_observations(vsmc_cuda_cv_filter *f,
+                                     const double *obs_x, const double *obs_y,
+                                     uint64_t n, int on_device);
+
+/* Enqueues device-to-host copies of step t's ESS, log-evidence increment and
+ * resampled flag (each pointer may be NULL).  With synchronize != 0 it waits
+ * and reports sticky device errors; otherwise the values are valid after
+ * the filter's stream reaches the copies. */
+int vsmc_cuda_cv_read_step(vsmc_cuda_cv_filter *f, uint64_t t, double *ess,
+                           double *logz_inc, int32_t *resampled,
+                           int synchronize);
+
+/* Kernel timing with CUDA events on the filter's stream.  While enabled,
+ * every step records events around the move kernel and around the whole
+ * step; vsmc_cuda_cv_timing returns the summed milliseconds of the move
+ * kernels and of whole steps, and the number of steps, since enabling (it
+ * synchronises).  *launches counts this library's kernel launches. */
+int vsmc_cuda_cv_set_timing(vsmc_cuda_cv_filter *f, int enable);
+int vsmc_cuda_cv_timing(vsmc_cuda_cv_filter *f, double *move_ms,
+                        double *step_ms, uint64_t *steps, uint64_t *launches);
+
+/* The workload's observation series: state (0,0,1,1), the configuration's
+ * constant-velocity dynamics, positions plus Student-t(nu)/scale noise; step
+ * t draws from Philox4x32-10 with key {obs_seed, 1} and counter
+ * {0, t, 0, cfg->stream_id} through std::normal_distribution.  Host arrays;
+ * truth (T x 4) may be NULL.  No device is used. */
+int vsmc_cuda_cv_simulate(const vsmc_cuda_cv_config *cfg, uint32_t obs_seed,
+                          uint64_t T, double *obs_x, double *obs_y,
+                          double *truth);
+
+/* Words drawn so far by the resample engine (Threefry4x64 offset). */
+int vsmc_cuda_cv_resample_words(vsmc_cuda_cv_filter *f, uint64_t *words);
+
+/* The filter's last copy_from vector (host, N int32) and whether the last
+ * step resampled.  Synchronises. */
+int vsmc_cuda_cv_copy_from(vsmc_cuda_cv_filter *f, int32_t *copy_from,
+                           int32_t *resampled);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VSMC_CUDA_H */

@@ -140,7 +140,7 @@ def ref():
         L.ref_weight_set.restype = C.c_double
         L.ref_cv_filter.argtypes = [C.c_int, C.c_int, _f64p, C.c_uint64, C.c_uint64,
                                     C.c_int, C.c_double, C.c_uint, C.c_uint,
-                                    _f64p, _f64p] + [C.c_void_p] * 9
+                                    _f64p, _f64p] + [C.c_void_p] * 10
         L.ref_cv_filter.restype = C.c_double
         L.ref_max_threads.restype = C.c_int
         _ref = L
@@ -324,9 +324,10 @@ def ref_cv_filter(N, T, scheme, obs_x, obs_y, seed=101, stream=0, threshold=0.5,
     lw = np.zeros(N) if want_state else None
     wu = np.zeros(1, np.uint64)
     sec = np.zeros(1)
+    r["step_seconds"] = np.zeros(T)
     p = np.asarray(param, np.float64)
     args = [r["ess"], r["resampled"], r["logz_inc"], r["mean_x"], r["mean_y"], st, lw,
-            wu, sec]
+            wu, sec, r["step_seconds"]]
     r["logz"] = ref().ref_cv_filter(backend, nthreads, p, N, T, scheme, threshold, seed,
                                     stream, ox, oy,
                                     *[a.ctypes.data if a is not None else None

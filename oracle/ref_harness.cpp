@@ -211,6 +211,7 @@ struct run_out {
     double *final_lw;
     uint64_t *words_used;
     double *seconds;
+    double *step_seconds;
 };
 
 template <template <typename> class StateB,
@@ -236,8 +237,16 @@ double run_filter (const cv_param &prm, std::size_t N, std::size_t T,
 
     auto t0 = std::chrono::steady_clock::now();
     sampler.initialize();
-    if (T > 1)
-        sampler.iterate(T - 1);
+    auto tp = std::chrono::steady_clock::now();
+    if (out && out->step_seconds)
+        out->step_seconds[0] = std::chrono::duration<double>(tp - t0).count();
+    for (std::size_t t = 1; t < T; ++t) {
+        sampler.iterate(1);
+        auto tn = std::chrono::steady_clock::now();
+        if (out && out->step_seconds)
+            out->step_seconds[t] = std::chrono::duration<double>(tn - tp).count();
+        tp = tn;
+    }
     auto t1 = std::chrono::steady_clock::now();
 
     if (out) {
@@ -375,17 +384,19 @@ double ref_weight_set (uint64_t N, const double *lw, const double *inc,
 // The CV Student-t bootstrap filter through Sampler<T>; backend 0 = OMP
 // (StateOMP/InitializeOMP/MoveOMP/MonitorEvalOMP), 1 = STD (std::thread),
 // 2 = SEQ.  nthreads > 0 sets the OpenMP thread count (OMP backend).
+// step_seconds (T entries, nullable): wall time of initialize and of each
+// iterate(1).
 double ref_cv_filter (int backend, int nthreads, const double *param,
         uint64_t N, uint64_t T, int scheme, double threshold, unsigned seed,
         unsigned stream, const double *ox, const double *oy,
         double *ess, int32_t *resampled, double *logz_inc, double *mean_x,
         double *mean_y, double *final_state, double *final_lw,
-        uint64_t *words_used, double *seconds)
+        uint64_t *words_used, double *seconds, double *step_seconds)
 {
     cv_param prm = {param[0], param[1], param[2], param[3], param[4],
         param[5], param[6]};
     run_out out = {ess, resampled, logz_inc, mean_x, mean_y, final_state,
-        final_lw, words_used, seconds};
+        final_lw, words_used, seconds, step_seconds};
     if (nthreads > 0)
         omp_set_num_threads(nthreads);
     switch (backend) {

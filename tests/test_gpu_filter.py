@@ -1,0 +1,118 @@
+"""The device CV Student-t filter against the oracle (the reference's own
+FP64 path on the same seed).
+
+FP64 form: resampling decisions, resample-engine words and copy_from are
+exact; log-evidence, ESS and the posterior-mean path agree to 1e-9 relative
+(the moves differ from glibc only through log() in the polar normals and
+exp() in the weights, a few ulps).  Mixed form (float move/weights, double
+scan and log-evidence): log-evidence within 1e-4 relative of the FP64 oracle
+on this 1000-particle run."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+RTOL_FP64 = 1e-9
+RTOL_MIXED = 1e-4
+
+
+@pytest.fixture(scope="module")
+def capi():
+    from vsmc_b200 import capi as C
+
+    C.lib()
+    return C
+
+
+def run_gpu(capi, N, T, scheme, ox, oy, form=0, seed=101, stream_id=0, threshold=0.5):
+    with capi.CVFilter(N, T, scheme=scheme, form=form, seed=seed, stream_id=stream_id,
+                       threshold=threshold) as f:
+        f.set_observations_host(ox, oy)
+        f.initialize()
+        f.iterate(T - 1)
+        h = f.history()
+        h["logz"] = f.log_evidence()
+        h["words_used"] = f.resample_words()
+        h["state"], h["lw"] = f.read_state()
+    return h
+
+
+def close(a, b, rtol):
+    return np.all(np.abs(a - b) <= rtol * np.maximum(np.abs(b), 1e-300) + 1e-12)
+
+
+@pytest.mark.parametrize("sch", range(6))
+def test_fp64_matches_golden(golden, capi, sch):
+    ox, oy = golden["cv_obs_x"], golden["cv_obs_y"]
+    h = run_gpu(capi, 1000, 100, sch, ox, oy)
+    assert np.array_equal(h["resampled"], golden[f"cv_s{sch}_resampled"])
+    assert h["words_used"] == int(golden[f"cv_s{sch}_words"])
+    assert abs(h["logz"] - golden[f"cv_s{sch}_logz"]) <= RTOL_FP64 * abs(golden[f"cv_s{sch}_logz"])
+    for k in ("ess", "logz_inc", "mean_x", "mean_y"):
+        assert close(h[k], golden[f"cv_s{sch}_{k}"], RTOL_FP64), k
+    if sch == 0:
+        assert close(h["state"], golden["cv_s0_state"], 1e-9)
+
+
+def test_fp64_second_stream(golden, capi):
+    ox, oy = golden["cv2_obs_x"], golden["cv2_obs_y"]
+    h = run_gpu(capi, 4096, 30, 3, ox, oy, seed=5, stream_id=3, threshold=0.8)
+    assert np.array_equal(h["resampled"], golden["cv2_resampled"])
+    assert abs(h["logz"] - golden["cv2_logz"]) <= RTOL_FP64 * abs(golden["cv2_logz"])
+    assert close(h["mean_x"], golden["cv2_mean_x"], RTOL_FP64)
+
+
+@pytest.mark.parametrize("N", [1 << 16])
+@pytest.mark.parametrize("sch", range(6))
+def test_fp64_large_against_oracle(capi, N, sch):
+    T = 40
+    ox, oy = O.cv_simulate(T, obs_seed=21)
+    r = O.cv_filter(N, T, sch, ox, oy, seed=3)
+    h = run_gpu(capi, N, T, sch, ox, oy, seed=3)
+    assert np.array_equal(h["resampled"], r["resampled"])
+    assert h["words_used"] == r["words_used"]
+    assert abs(h["logz"] - r["logz"]) <= RTOL_FP64 * abs(r["logz"])
+    assert close(h["ess"], r["ess"], RTOL_FP64)
+
+
+@pytest.mark.parametrize("sch", [0, 3])
+def test_mixed_form(golden, capi, sch):
+    ox, oy = golden["cv_obs_x"], golden["cv_obs_y"]
+    h = run_gpu(capi, 1000, 100, sch, ox, oy, form=capi.MIXED)
+    ref = float(golden[f"cv_s{sch}_logz"])
+    err = abs(h["logz"] - ref) / abs(ref)
+    print(f"mixed form scheme {sch}: logZ {h['logz']:.10f} vs FP64 oracle {ref:.10f}, "
+          f"rel err {err:.3e}")
+    assert err <= RTOL_MIXED
+
+
+def test_repeatable(golden, capi):
+    ox, oy = golden["cv_obs_x"], golden["cv_obs_y"]
+    a = run_gpu(capi, 3000, 50, 0, ox, oy)
+    b = run_gpu(capi, 3000, 50, 0, ox, oy)
+    assert a["logz"] == b["logz"] and np.array_equal(a["ess"], b["ess"])
+
+
+def test_degenerate_observation(capi):
+    """A NaN observation makes every likelihood NaN: the step reports
+    VSMC_CUDA_EDEGENERATE instead of silently producing NaN weights."""
+    ox, oy = O.cv_simulate(5, obs_seed=1)
+    ox[3] = np.nan
+    with capi.CVFilter(1024, 5) as f:
+        f.set_observations_host(ox, oy)
+        f.initialize()
+        f.iterate(4)
+        with pytest.raises(capi.VsmcCudaError) as e:
+            f.synchronize()
+        assert e.value.status == capi.EDEGENERATE
+
+
+def test_iterate_beyond_observations(capi):
+    ox, oy = O.cv_simulate(5, obs_seed=1)
+    with capi.CVFilter(1024, 10) as f:
+        f.set_observations_host(ox, oy)
+        f.initialize()
+        with pytest.raises(capi.VsmcCudaError):
+            f.iterate(5)

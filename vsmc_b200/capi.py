@@ -1,0 +1,310 @@
+"""ctypes binding of libvsmc_cuda (the C ABI declared in include/vsmc_cuda.h).
+
+This is the Python host mirror used by the tests and bench.py: it calls the
+sm_100a kernels through the C ABI with raw device pointers and raises
+``VsmcCudaError`` on any non-zero status.  There is no CPU path: loading
+fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libvsmc_cuda.so")
+
+OK, EINVAL, ENOMEM, EDEGENERATE, ETIMEOUT, ECUDA = range(6)
+
+# vsmc::ResampleScheme values (include/vsmc/resample/common.hpp:124-131)
+Multinomial, Residual, Stratified, Systematic, ResidualStratified, ResidualSystematic = range(6)
+SCHEME_NAMES = ("Multinomial", "Residual", "Stratified", "Systematic",
+                "ResidualStratified", "ResidualSystematic")
+FP64, MIXED = 0, 1
+
+
+class VsmcCudaError(RuntimeError):
+    def __init__(self, status: int, where: str, message: str):
+        super().__init__(f"{where}: status {status} ({message})")
+        self.status = status
+
+
+class CVConfig(C.Structure):
+    _fields_ = [
+        ("N", C.c_uint64), ("T_max", C.c_uint64), ("scheme", C.c_int),
+        ("form", C.c_int), ("threshold", C.c_double), ("seed", C.c_uint32),
+        ("stream_id", C.c_uint32), ("dt", C.c_double), ("sd_pos", C.c_double),
+        ("sd_vel", C.c_double), ("sd_pos0", C.c_double), ("sd_vel0", C.c_double),
+        ("scale", C.c_double), ("nu", C.c_double)]
+
+
+class ThreefryState(C.Structure):
+    _fields_ = [("key", C.c_uint64 * 4), ("ctr", C.c_uint64 * 4),
+                ("offset", C.c_uint64)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libvsmc_cuda.so (built by vsmc_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m vsmc_b200.build` "
+            "(nvcc, sm_100a); there is no CPU fallback")
+    L = C.CDLL(LIB_PATH)
+    vp, u64, i32, f64 = C.c_void_p, C.c_uint64, C.c_int, C.c_double
+    L.vsmc_cuda_last_error.restype = C.c_char_p
+    L.vsmc_cuda_status_string.restype = C.c_char_p
+    L.vsmc_cuda_status_string.argtypes = [i32]
+    L.vsmc_cuda_abi_version.restype = i32
+    L.vsmc_cuda_philox4x32_words.argtypes = [vp, vp, u64, u64, vp, vp]
+    L.vsmc_cuda_threefry4x64_words.argtypes = [vp, vp, u64, u64, vp, vp]
+    L.vsmc_cuda_weight_add_log.argtypes = [u64, vp, vp, vp, C.POINTER(f64), vp]
+    L.vsmc_cuda_resample_workspace_size.restype = C.c_size_t
+    L.vsmc_cuda_resample_workspace_size.argtypes = [u64]
+    L.vsmc_cuda_resample.argtypes = [i32, u64, vp, vp, u64, C.POINTER(ThreefryState),
+                                     vp, vp, vp, C.c_size_t, vp]
+    L.vsmc_cuda_copy_f64.argtypes = [u64, C.c_uint32, vp, vp, vp, vp]
+    L.vsmc_cuda_cv_config_default.argtypes = [C.POINTER(CVConfig)]
+    L.vsmc_cuda_cv_config_default.restype = None
+    L.vsmc_cuda_cv_device_bytes.argtypes = [C.POINTER(CVConfig)]
+    L.vsmc_cuda_cv_device_bytes.restype = C.c_size_t
+    L.vsmc_cuda_cv_create.argtypes = [C.POINTER(CVConfig), vp, C.POINTER(vp)]
+    L.vsmc_cuda_cv_destroy.argtypes = [vp]
+    L.vsmc_cuda_cv_set_observations.argtypes = [vp, vp, vp, u64, i32]
+    L.vsmc_cuda_cv_initialize.argtypes = [vp]
+    L.vsmc_cuda_cv_iterate.argtypes = [vp, u64]
+    L.vsmc_cuda_cv_synchronize.argtypes = [vp]
+    L.vsmc_cuda_cv_iter_size.argtypes = [vp, C.POINTER(u64)]
+    L.vsmc_cuda_cv_history.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.vsmc_cuda_cv_log_evidence.argtypes = [vp, C.POINTER(f64)]
+    L.vsmc_cuda_cv_read_state.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.vsmc_cuda_cv_resample_words.argtypes = [vp, C.POINTER(u64)]
+    L.vsmc_cuda_cv_copy_from.argtypes = [vp, vp, vp]
+    L.vsmc_cuda_cv_append_observations.argtypes = [vp, vp, vp, u64, i32]
+    L.vsmc_cuda_cv_read_step.argtypes = [vp, u64, vp, vp, vp, i32]
+    L.vsmc_cuda_cv_set_timing.argtypes = [vp, i32]
+    L.vsmc_cuda_cv_timing.argtypes = [vp, C.POINTER(f64), C.POINTER(f64), C.POINTER(u64),
+                                      C.POINTER(u64)]
+    L.vsmc_cuda_cv_simulate.argtypes = [C.POINTER(CVConfig), C.c_uint32, u64, vp, vp, vp]
+    _lib = L
+    return L
+
+
+def check(status: int, where: str) -> None:
+    if status != OK:
+        msg = lib().vsmc_cuda_last_error().decode(errors="replace")
+        raise VsmcCudaError(status, where, msg)
+
+
+def _np_ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+# --------------------------------------------------------------- RNG -------
+
+def philox4x32_words(key, ctr, skip, n, out_ptr, stream=None):
+    k = (C.c_uint32 * 2)(*key)
+    c = (C.c_uint32 * 4)(*ctr)
+    check(lib().vsmc_cuda_philox4x32_words(k, c, skip, n, out_ptr, stream),
+          "vsmc_cuda_philox4x32_words")
+
+
+def threefry4x64_words(key, ctr, skip, n, out_ptr, stream=None):
+    k = (C.c_uint64 * 4)(*key)
+    c = (C.c_uint64 * 4)(*ctr)
+    check(lib().vsmc_cuda_threefry4x64_words(k, c, skip, n, out_ptr, stream),
+          "vsmc_cuda_threefry4x64_words")
+
+
+# ----------------------------------------------------------- weights -------
+
+def weight_add_log(N, lw_ptr, w_ptr=None, inc_ptr=None, stream=None) -> float:
+    ess = C.c_double(0.0)
+    check(lib().vsmc_cuda_weight_add_log(N, lw_ptr, w_ptr, inc_ptr, C.byref(ess), stream),
+          "vsmc_cuda_weight_add_log")
+    return ess.value
+
+
+# ---------------------------------------------------------- resample -------
+
+def resample_workspace_size(N) -> int:
+    return int(lib().vsmc_cuda_resample_workspace_size(N))
+
+
+def threefry_state(seed=0, key=None, ctr=(0, 0, 0, 0), offset=0) -> ThreefryState:
+    st = ThreefryState()
+    k = key if key is not None else (seed, 0, 0, 0)
+    for i in range(4):
+        st.key[i] = k[i]
+        st.ctr[i] = ctr[i]
+    st.offset = offset
+    return st
+
+
+def resample(scheme, N, weight_ptr, rng: ThreefryState, rep_ptr, cf_ptr, ws_ptr, ws_bytes,
+             uniforms_ptr=None, n_uniforms=0, stream=None) -> int:
+    """Returns the number of engine words drawn; rng.offset advances."""
+    before = rng.offset
+    check(lib().vsmc_cuda_resample(scheme, N, weight_ptr, uniforms_ptr, n_uniforms,
+                                   C.byref(rng), rep_ptr, cf_ptr, ws_ptr, ws_bytes, stream),
+          "vsmc_cuda_resample")
+    return int(rng.offset - before)
+
+
+def copy_f64(N, dim, src_ptr, dst_ptr, cf_ptr, stream=None):
+    check(lib().vsmc_cuda_copy_f64(N, dim, src_ptr, dst_ptr, cf_ptr, stream),
+          "vsmc_cuda_copy_f64")
+
+
+# -------------------------------------------------------- CV filter -------
+
+def cv_config(**kw) -> CVConfig:
+    c = CVConfig()
+    lib().vsmc_cuda_cv_config_default(C.byref(c))
+    for k, v in kw.items():
+        if not hasattr(c, k):
+            raise KeyError(k)
+        setattr(c, k, v)
+    return c
+
+
+def cv_simulate(T, obs_seed, stream_id=0, want_truth=False, **params):
+    """The workload's observation series (host computation, no device)."""
+    import numpy as np
+    c = cv_config(stream_id=stream_id, **params)
+    ox, oy = np.zeros(T), np.zeros(T)
+    truth = np.zeros((T, 4))
+    check(lib().vsmc_cuda_cv_simulate(C.byref(c), obs_seed, T, ox.ctypes.data,
+                                      oy.ctypes.data, truth.ctypes.data),
+          "vsmc_cuda_cv_simulate")
+    return (ox, oy, truth) if want_truth else (ox, oy)
+
+
+class CVFilter:
+    """The constant-velocity Student-t filter as a device-resident Sampler:
+    ``initialize()`` and ``iterate(n)`` mirror vsmc::Sampler (core/sampler.hpp:
+    450-483); histories mirror ess_history / resampled_history / Monitor."""
+
+    def __init__(self, N, T_max, scheme=Multinomial, form=FP64, threshold=0.5, seed=101,
+                 stream_id=0, stream=None, **params):
+        self.cfg = cv_config(N=N, T_max=T_max, scheme=scheme, form=form,
+                             threshold=threshold, seed=seed, stream_id=stream_id, **params)
+        self.N = N
+        self.stream = stream
+        h = C.c_void_p()
+        check(lib().vsmc_cuda_cv_create(C.byref(self.cfg), stream, C.byref(h)),
+              "vsmc_cuda_cv_create")
+        self.h = h
+
+    @staticmethod
+    def device_bytes(**kw) -> int:
+        c = cv_config(**kw)
+        return int(lib().vsmc_cuda_cv_device_bytes(C.byref(c)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            check(lib().vsmc_cuda_cv_destroy(self.h), "vsmc_cuda_cv_destroy")
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_observations(self, ox_ptr, oy_ptr, T, on_device):
+        check(lib().vsmc_cuda_cv_set_observations(self.h, ox_ptr, oy_ptr, T,
+                                                  1 if on_device else 0),
+              "vsmc_cuda_cv_set_observations")
+
+    def set_observations_host(self, ox, oy):
+        """numpy float64 arrays; copied before returning."""
+        import numpy as np
+        self._ox = np.ascontiguousarray(ox, np.float64)
+        self._oy = np.ascontiguousarray(oy, np.float64)
+        self.set_observations(self._ox.ctypes.data, self._oy.ctypes.data, self._ox.size, False)
+        self.synchronize()
+
+    def initialize(self):
+        check(lib().vsmc_cuda_cv_initialize(self.h), "vsmc_cuda_cv_initialize")
+
+    def iterate(self, num=1):
+        check(lib().vsmc_cuda_cv_iterate(self.h, num), "vsmc_cuda_cv_iterate")
+
+    def synchronize(self):
+        check(lib().vsmc_cuda_cv_synchronize(self.h), "vsmc_cuda_cv_synchronize")
+
+    def iter_size(self) -> int:
+        n = C.c_uint64()
+        check(lib().vsmc_cuda_cv_iter_size(self.h, C.byref(n)), "vsmc_cuda_cv_iter_size")
+        return int(n.value)
+
+    def history(self):
+        import numpy as np
+        T = self.iter_size()
+        r = dict(ess=np.zeros(T), resampled=np.zeros(T, np.int32), logz_inc=np.zeros(T),
+                 mean_x=np.zeros(T), mean_y=np.zeros(T))
+        check(lib().vsmc_cuda_cv_history(self.h, *[_np_ptr(r[k]) for k in
+                                                   ("ess", "resampled", "logz_inc",
+                                                    "mean_x", "mean_y")]),
+              "vsmc_cuda_cv_history")
+        return r
+
+    def log_evidence(self) -> float:
+        v = C.c_double()
+        check(lib().vsmc_cuda_cv_log_evidence(self.h, C.byref(v)), "vsmc_cuda_cv_log_evidence")
+        return v.value
+
+    def read_state(self):
+        import numpy as np
+        s = np.zeros((4, self.N))
+        lw = np.zeros(self.N)
+        check(lib().vsmc_cuda_cv_read_state(self.h, _np_ptr(s[0]), _np_ptr(s[1]),
+                                            _np_ptr(s[2]), _np_ptr(s[3]), _np_ptr(lw)),
+              "vsmc_cuda_cv_read_state")
+        return s, lw
+
+    def append_observations(self, ox_ptr, oy_ptr, n, on_device=False):
+        check(lib().vsmc_cuda_cv_append_observations(self.h, ox_ptr, oy_ptr, n,
+                                                     1 if on_device else 0),
+              "vsmc_cuda_cv_append_observations")
+
+    def read_step(self, t, ess_ptr=None, logz_ptr=None, res_ptr=None, synchronize=True):
+        check(lib().vsmc_cuda_cv_read_step(self.h, t, ess_ptr, logz_ptr, res_ptr,
+                                           1 if synchronize else 0),
+              "vsmc_cuda_cv_read_step")
+
+    def set_timing(self, enable=True):
+        check(lib().vsmc_cuda_cv_set_timing(self.h, 1 if enable else 0),
+              "vsmc_cuda_cv_set_timing")
+
+    def timing(self):
+        """(move_ms, step_ms, steps, launches) summed since set_timing(True)."""
+        mv, st, n, la = C.c_double(), C.c_double(), C.c_uint64(), C.c_uint64()
+        check(lib().vsmc_cuda_cv_timing(self.h, C.byref(mv), C.byref(st), C.byref(n),
+                                         C.byref(la)), "vsmc_cuda_cv_timing")
+        return mv.value, st.value, int(n.value), int(la.value)
+
+    def resample_words(self) -> int:
+        v = C.c_uint64()
+        check(lib().vsmc_cuda_cv_resample_words(self.h, C.byref(v)),
+              "vsmc_cuda_cv_resample_words")
+        return int(v.value)
+
+    def copy_from(self):
+        import numpy as np
+        cf = np.zeros(self.N, np.int32)
+        r = C.c_int32()
+        check(lib().vsmc_cuda_cv_copy_from(self.h, _np_ptr(cf), C.byref(r)),
+              "vsmc_cuda_cv_copy_from")
+        return cf, bool(r.value)
