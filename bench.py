@@ -250,6 +250,7 @@ def main():
     ms = max_over_ranks(e0.elapsed_time(e1))
     f.synchronize()
     hist = f.history()
+    logz = f.log_evidence()  # of this run (initialize() keeps the engine)
     value = world * N * K / (ms / 1e3)
     resampled = hist["resampled"][1 + W:]
     n_res = int(resampled.sum())
@@ -290,7 +291,6 @@ def main():
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_logz = g.log_evidence()
     g.close()
-    logz = f.log_evidence()
     f.close()
     e2e = world * N * K / e2e_s
 

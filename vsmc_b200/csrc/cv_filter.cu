@@ -37,12 +37,17 @@ struct FilterCtl {
     long long monitor_done; // step whose gathered monitor is already written
 };
 
+// Per-tile statistics of the new log-weights: online log-sum-exp (m, s1, s2),
+// the weighted position sums (sx, sy) and the sums of the gathered previous
+// positions (gx, gy) for the monitor of a resampled step.
 struct TileStats {
     double m, s1, s2, sx, sy, gx, gy, pad;
 };
 
 struct CVParam {
     double dt, sd_pos, sd_vel, sd_pos0, sd_vel0, scale, nu;
+    double inv_nu; // 1 / nu
+    double coef;   // -(nu + 1) / 2
 };
 
 template <typename Real>
@@ -76,22 +81,38 @@ struct Vec<float> {
 
 __device__ __forceinline__ double plus0(double v) { return __dadd_rn(v, 0.0); }
 
-// One particle, FP64 form: cv_move::move_state / cv_init::initialize_state
-// with the reference's evaluation order.
-template <bool Init>
-__device__ __forceinline__ void cv_particle(const CVParam &p, uint32_t iter,
-                                            uint32_t id, uint32_t stream,
-                                            uint32_t k0, uint32_t k1,
-                                            double &x, double &y, double &vx,
-                                            double &vy)
+__device__ __forceinline__ PhiloxStream particle_stream(uint32_t iter,
+                                                        uint32_t id,
+                                                        uint32_t stream,
+                                                        uint32_t k0,
+                                                        uint32_t k1)
 {
     PhiloxStream s;
     s.ctr = make_uint4(0u, iter, id, stream);
     s.k0 = k0;
     s.k1 = k1;
-    double a, b, c, d;
-    polar_pair_f64(s, a, b);
-    polar_pair_f64(s, c, d);
+    return s;
+}
+
+// FP64 form: cv_move::move_state / cv_init::initialize_state
+// (pf_smp.hpp:150-173, 207-238).  The two polar points are drawn first and
+// their transforms evaluated together (independent chains for the FP64
+// pipe); the state update keeps the reference's evaluation order.
+template <bool Init>
+__device__ __forceinline__ void cv_particle(const CVParam &p, uint32_t iter,
+                                            uint32_t id, uint32_t stream,
+                                            uint32_t k0, uint32_t k1,
+                                            double &x, double &y, double &vx,
+                                            double &vy, double, double)
+{
+    PhiloxStream s = particle_stream(iter, id, stream, k0, k1);
+    double x1, y1, q1, x2, y2, q2;
+    polar_accept(s, x1, y1, q1);
+    polar_accept(s, x2, y2, q2);
+    const double m1 = polar_mult_f64(q1);
+    const double m2 = polar_mult_f64(q2);
+    const double a = __dmul_rn(y1, m1), b = __dmul_rn(x1, m1);
+    const double c = __dmul_rn(y2, m2), d = __dmul_rn(x2, m2);
     if (Init) {
         x = plus0(__dmul_rn(a, p.sd_pos0));
         y = plus0(__dmul_rn(b, p.sd_pos0));
@@ -109,60 +130,62 @@ __device__ __forceinline__ void cv_particle(const CVParam &p, uint32_t iter,
     }
 }
 
-// cv_state::log_likelihood (pf_smp.hpp:96-112).
+// cv_state::log_likelihood (pf_smp.hpp:96-112): the two Student-t terms
+// share one log, log(1 + a) + log(1 + b) = log((1 + a)(1 + b)).
 __device__ __forceinline__ double cv_loglik(const CVParam &p, double x,
                                             double y, double ox, double oy)
 {
-    double lx = __dmul_rn(p.scale, __dadd_rn(x, -ox));
-    double ly = __dmul_rn(p.scale, __dadd_rn(y, -oy));
-    lx = log(__dadd_rn(1.0, __ddiv_rn(__dmul_rn(lx, lx), p.nu)));
-    ly = log(__dadd_rn(1.0, __ddiv_rn(__dmul_rn(ly, ly), p.nu)));
-    return __dmul_rn(__dmul_rn(-0.5, __dadd_rn(p.nu, 1.0)),
-                     __dadd_rn(lx, ly));
+    const double lx = p.scale * (x - ox);
+    const double ly = p.scale * (y - oy);
+    const double a = lx * lx * p.inv_nu, b = ly * ly * p.inv_nu;
+    return p.coef * log((1.0 + a) * (1.0 + b));
 }
 
-// Mixed form: same stream consumption, float transform and state.
+// Mixed form: the same stream consumption; float transforms and state.  The
+// stored positions are offsets from the step's observation (x - ox, y - oy)
+// so that float keeps its precision where the likelihood looks (the
+// residual); (shx, shy) = previous observation minus this one, in double
+// rounded once, re-anchors the loaded offsets.
 template <bool Init>
 __device__ __forceinline__ void cv_particle(const CVParam &p, uint32_t iter,
                                             uint32_t id, uint32_t stream,
                                             uint32_t k0, uint32_t k1, float &x,
-                                            float &y, float &vx, float &vy)
+                                            float &y, float &vx, float &vy,
+                                            double shx, double shy)
 {
-    PhiloxStream s;
-    s.ctr = make_uint4(0u, iter, id, stream);
-    s.k0 = k0;
-    s.k1 = k1;
-    float a, b, c, d;
-    polar_pair_f32(s, a, b);
-    polar_pair_f32(s, c, d);
+    PhiloxStream s = particle_stream(iter, id, stream, k0, k1);
+    double x1, y1, q1, x2, y2, q2;
+    polar_accept(s, x1, y1, q1);
+    polar_accept(s, x2, y2, q2);
     if (Init) {
-        x = a * (float)p.sd_pos0;
-        y = b * (float)p.sd_pos0;
-        vx = c * (float)p.sd_vel0;
-        vy = d * (float)p.sd_vel0;
+        // once per run: the prior in double, then stored as float offsets
+        const double m1 = polar_mult_f64(q1), m2 = polar_mult_f64(q2);
+        x = (float)(y1 * m1 * p.sd_pos0 + shx);
+        y = (float)(x1 * m1 * p.sd_pos0 + shy);
+        vx = (float)(y2 * m2 * p.sd_vel0);
+        vy = (float)(x2 * m2 * p.sd_vel0);
     } else {
+        const float m1 = polar_mult_f32(q1), m2 = polar_mult_f32(q2);
         const float dt = (float)p.dt;
-        x = x + (a * (float)p.sd_pos + dt * vx);
-        y = y + (b * (float)p.sd_pos + dt * vy);
-        vx = vx + c * (float)p.sd_vel;
-        vy = vy + d * (float)p.sd_vel;
+        x = (x + (float)shx) + ((float)y1 * m1 * (float)p.sd_pos + dt * vx);
+        y = (y + (float)shy) + ((float)x1 * m1 * (float)p.sd_pos + dt * vy);
+        vx = vx + (float)y2 * m2 * (float)p.sd_vel;
+        vy = vy + (float)x2 * m2 * (float)p.sd_vel;
     }
 }
 
+// Mixed form likelihood on the anchored offsets (x, y are x - ox, y - oy).
 __device__ __forceinline__ float cv_loglik(const CVParam &p, float x, float y,
-                                           double ox, double oy)
+                                           double, double)
 {
-    const float s = (float)p.scale, nu = (float)p.nu;
-    const float lx = s * (x - (float)ox);
-    const float ly = s * (y - (float)oy);
-    return -0.5f * (nu + 1.0f) * (log1pf(lx * lx / nu) + log1pf(ly * ly / nu));
+    const float s = (float)p.scale, inv = (float)p.inv_nu;
+    const float lx = s * x, ly = s * y;
+    const float a = lx * lx * inv, b = ly * ly * inv;
+    return (float)p.coef * log1pf(a + b + a * b);
 }
 
 __device__ __forceinline__ double lse_exp(double v) { return exp(v); }
-__device__ __forceinline__ double lse_exp(float v)
-{
-    return (double)expf(v);
-}
+__device__ __forceinline__ double lse_exp(float v) { return (double)expf(v); }
 
 // Accumulate one particle into the thread's online LSE state; `Real`
 // selects the exp precision.
@@ -186,19 +209,45 @@ __device__ __forceinline__ void lse_add(LseAcc &a, Real lw, Real x, Real y)
     a.sy += e * (double)y;
 }
 
+__device__ __forceinline__ void warp_merge(LseAcc &a, double &gx, double &gy,
+                                           unsigned width)
+{
+    for (unsigned o = width / 2; o > 0; o >>= 1) {
+        a.merge(shfl_xor(a, (int)o));
+        gx += __shfl_xor_sync(0xffffffffu, gx, o);
+        gy += __shfl_xor_sync(0xffffffffu, gy, o);
+    }
+}
+
+#ifndef VSMC_MOVE_MIN_BLOCKS
+#define VSMC_MOVE_MIN_BLOCKS 3
+#endif
+
 template <typename Real, bool Init>
-__global__ void __launch_bounds__(kThreads) k_cv_move(MoveArgs<Real> a)
+__global__ void __launch_bounds__(kThreads, VSMC_MOVE_MIN_BLOCKS)
+k_cv_move(MoveArgs<Real> a)
 {
     constexpr int V = Vec<Real>::n;
     constexpr int NV = kItems / V;
+    constexpr bool Anchored = sizeof(Real) == 4;
     typedef typename Vec<Real>::type VT;
-    __shared__ LseAcc sh_acc[kThreads / 32];
-    __shared__ double sh_g[2][kThreads / 32];
+    constexpr int NW = kThreads / 32;
+    // double-buffered warp partials: one barrier per tile
+    __shared__ LseAcc sh_acc[2][NW];
+    __shared__ double sh_g[2][2][NW];
 
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int gather = Init ? 0 : a.ctl->resampled;
     const Real mprev = Init || gather ? Real(0) : (Real)a.ctl->lw_max;
     const double ox = a.obs_x[a.iter], oy = a.obs_y[a.iter];
+    // re-anchoring of the mixed form's offsets
+    double shx = 0.0, shy = 0.0;
+    if (Anchored) {
+        shx = Init ? -ox : a.obs_x[a.iter - 1] - ox;
+        shy = Init ? -oy : a.obs_y[a.iter - 1] - oy;
+    }
     const long long N = a.N;
+    int buf = 0;
 
     for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
         const long long base = (long long)tile * kTile;
@@ -207,7 +256,8 @@ __global__ void __launch_bounds__(kThreads) k_cv_move(MoveArgs<Real> a)
         double gx = 0.0, gy = 0.0;
 #pragma unroll 1
         for (int v = 0; v < NV; ++v) {
-            const long long p0 = base + ((long long)v * kThreads + threadIdx.x) * V;
+            const long long p0 =
+                base + ((long long)v * kThreads + threadIdx.x) * V;
             Real s[4][V];
             Real lwv[V];
             const bool full = p0 + V <= N;
@@ -233,7 +283,7 @@ __global__ void __launch_bounds__(kThreads) k_cv_move(MoveArgs<Real> a)
                     const long long i = p0 + e;
                     if (i < N) {
                         long long src = i;
-                        if (gather) { // clamped: a bad index never leaves [0, N)
+                        if (gather) { // clamped: never leaves [0, N)
                             src = a.copy_from[i];
                             src = src < 0 ? 0 : (src >= N ? N - 1 : src);
                         }
@@ -255,7 +305,7 @@ __global__ void __launch_bounds__(kThreads) k_cv_move(MoveArgs<Real> a)
                 if (i < N) {
                     cv_particle<Init>(a.p, a.iter, (uint32_t)i, a.stream, a.k0,
                                       a.k1, s[0][e], s[1][e], s[2][e],
-                                      s[3][e]);
+                                      s[3][e], shx, shy);
                     const Real inc = cv_loglik(a.p, s[0][e], s[1][e], ox, oy);
                     // lw += -max (normalize_log_weight), then += inc
                     lwn[e] = Init ? inc : (lwv[e] - mprev) + inc;
@@ -291,32 +341,38 @@ __global__ void __launch_bounds__(kThreads) k_cv_move(MoveArgs<Real> a)
                 }
             }
         }
-        const LseAcc r = block_reduce_lse(acc, sh_acc);
-        gx = warp_sum(gx);
-        gy = warp_sum(gy);
-        if ((threadIdx.x & 31) == 0) {
-            sh_g[0][threadIdx.x >> 5] = gx;
-            sh_g[1][threadIdx.x >> 5] = gy;
+        warp_merge(acc, gx, gy, 32);
+        if (lane == 0) {
+            sh_acc[buf][wid] = acc;
+            sh_g[buf][0][wid] = gx;
+            sh_g[buf][1][wid] = gy;
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (wid == 0) {
+            LseAcc r;
             double tx = 0.0, ty = 0.0;
-            for (int w = 0; w < kThreads / 32; ++w) {
-                tx += sh_g[0][w];
-                ty += sh_g[1][w];
+            if (lane < NW) {
+                r = sh_acc[buf][lane];
+                tx = sh_g[buf][0][lane];
+                ty = sh_g[buf][1][lane];
+            } else {
+                r.init();
             }
-            TileStats ts;
-            ts.m = r.m;
-            ts.s1 = r.s1;
-            ts.s2 = r.s2;
-            ts.sx = r.sx;
-            ts.sy = r.sy;
-            ts.gx = tx;
-            ts.gy = ty;
-            ts.pad = 0.0;
-            a.tile_stats[tile] = ts;
+            warp_merge(r, tx, ty, NW);
+            if (lane == 0) {
+                TileStats ts;
+                ts.m = r.m;
+                ts.s1 = r.s1;
+                ts.s2 = r.s2;
+                ts.sx = r.sx;
+                ts.sy = r.sy;
+                ts.gx = tx;
+                ts.gy = ty;
+                ts.pad = 0.0;
+                a.tile_stats[tile] = ts;
+            }
         }
-        __syncthreads();
+        buf ^= 1;
     }
 }
 
@@ -328,6 +384,9 @@ struct FinalizeArgs {
     double threshold;
     long long t;
     int init;
+    int anchored;
+    const double *obs_x;
+    const double *obs_y;
     double *hist_ess;
     int32_t *hist_resampled;
     double *hist_logz_inc;
@@ -340,56 +399,78 @@ struct FinalizeArgs {
     EngineRef eng;
 };
 
-// One CTA.  Deterministic: each thread folds a contiguous run of tiles, the
-// block folds the threads in a fixed tree.
-__global__ void __launch_bounds__(kSpineThreads) k_cv_finalize(FinalizeArgs a)
+constexpr int kFinalThreads = 1024;
+
+// One CTA, deterministic (contiguous runs of tiles per thread, fixed
+// reduction trees): pass 1 the global maximum M, pass 2 the rescaled sums
+// s1_t exp(m_t - M) etc. (independent exponentials, no serial chain), then
+// the decisions of Sampler::do_resample and the weight spine.
+__global__ void __launch_bounds__(kFinalThreads) k_cv_finalize(FinalizeArgs a)
 {
-    __shared__ LseAcc sh_acc[kSpineThreads / 32];
-    __shared__ double sh_g[2][kSpineThreads / 32];
-    __shared__ double sh_spine[kSpineThreads / 32];
+    constexpr int NW = kFinalThreads / 32;
+    __shared__ double sh[7][NW];
+    __shared__ double sh_spine[NW];
     __shared__ int sh_res;
+    __shared__ double sh_M, sh_coeff;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int per = (a.ntiles + blockDim.x - 1) / blockDim.x;
     const int b = threadIdx.x * per, e = min(b + per, a.ntiles);
-    LseAcc acc;
-    acc.init();
-    double gx = 0.0, gy = 0.0;
+    // pass 1: maximum (NaN propagates)
+    double m = -INFINITY;
     for (int t = b; t < e; ++t) {
-        LseAcc o;
-        o.m = a.ts[t].m;
-        o.s1 = a.ts[t].s1;
-        o.s2 = a.ts[t].s2;
-        o.sx = a.ts[t].sx;
-        o.sy = a.ts[t].sy;
-        if (o.s1 != o.s1)
-            acc.s1 = o.s1;
-        else
-            acc.merge(o);
-        gx += a.ts[t].gx;
-        gy += a.ts[t].gy;
+        const double mt = a.ts[t].m, st = a.ts[t].s1;
+        m = (mt != mt || st != st) ? NAN : (m != m ? m : fmax(m, mt));
     }
-    const LseAcc r = block_reduce_lse(acc, sh_acc);
-    gx = warp_sum(gx);
-    gy = warp_sum(gy);
-    if ((threadIdx.x & 31) == 0) {
-        sh_g[0][threadIdx.x >> 5] = gx;
-        sh_g[1][threadIdx.x >> 5] = gy;
+    for (int o = 16; o > 0; o >>= 1) {
+        const double q = __shfl_xor_sync(0xffffffffu, m, o);
+        m = (q != q || m != m) ? NAN : fmax(m, q);
+    }
+    if (lane == 0)
+        sh[0][wid] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = -INFINITY;
+        for (int w = 0; w < NW; ++w)
+            r = (sh[0][w] != sh[0][w] || r != r) ? NAN : fmax(r, sh[0][w]);
+        sh_M = r;
+    }
+    __syncthreads();
+    const double M = sh_M;
+    // pass 2: sums rescaled to M
+    double v[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int t = b; t < e; ++t) {
+        const TileStats ts = a.ts[t];
+        const double f = ts.m == -INFINITY ? 0.0 : exp(ts.m - M);
+        v[0] += ts.s1 * f;
+        v[1] += ts.s2 * f * f;
+        v[2] += ts.sx * f;
+        v[3] += ts.sy * f;
+        v[4] += ts.gx;
+        v[5] += ts.gy;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        v[k] = warp_sum(v[k]);
+        if (lane == 0)
+            sh[k][wid] = v[k];
     }
     __syncthreads();
     FilterCtl *c = a.ctl;
     const double Nd = (double)a.N;
     if (threadIdx.x == 0) {
-        double tx = 0.0, ty = 0.0;
-        for (int w = 0; w < kSpineThreads / 32; ++w) {
-            tx += sh_g[0][w];
-            ty += sh_g[1][w];
-        }
+        double r[6] = {0, 0, 0, 0, 0, 0};
+        for (int w = 0; w < NW; ++w)
+            for (int k = 0; k < 6; ++k)
+                r[k] += sh[k][w];
+        const double S1 = r[0], S2 = r[1];
         // monitor of the previous step, gathered by this move
         if (!a.init && c->resampled && c->monitor_done != a.t - 1) {
-            a.hist_mean_x[a.t - 1] = tx / Nd;
-            a.hist_mean_y[a.t - 1] = ty / Nd;
+            const double ax = a.anchored ? a.obs_x[a.t - 1] : 0.0;
+            const double ay = a.anchored ? a.obs_y[a.t - 1] : 0.0;
+            a.hist_mean_x[a.t - 1] = ax + r[4] / Nd;
+            a.hist_mean_y[a.t - 1] = ay + r[5] / Nd;
             c->monitor_done = a.t - 1;
         }
-        const double M = r.m, S1 = r.s1, S2 = r.s2;
         const double s1prev = (a.init || c->resampled) ? Nd : c->s1;
         int res = 0;
         double ess = S1 * S1 / S2;
@@ -412,18 +493,21 @@ __global__ void __launch_bounds__(kSpineThreads) k_cv_finalize(FinalizeArgs a)
         c->ess = ess;
         c->resampled = res;
         if (!res) {
-            a.hist_mean_x[a.t] = r.sx / S1;
-            a.hist_mean_y[a.t] = r.sy / S1;
+            const double ax = a.anchored ? a.obs_x[a.t] : 0.0;
+            const double ay = a.anchored ? a.obs_y[a.t] : 0.0;
+            a.hist_mean_x[a.t] = ax + r[2] / S1;
+            a.hist_mean_y[a.t] = ay + r[3] / S1;
         }
         a.rctl->active = res;
         sh_res = res;
+        sh_coeff = __ddiv_rn(1.0, S1);
     }
     __syncthreads();
     if (!sh_res || a.residual)
         return;
     // weight spine for the resampling scan: tile t holds
     // exp(m_t - M) * s1_t / S1 of the normalised weight mass
-    const double M = c->lw_max, coeff = __ddiv_rn(1.0, c->s1);
+    const double coeff = sh_coeff;
     double run = 0.0;
     for (int t = b; t < e; ++t)
         run += exp(a.ts[t].m - M) * a.ts[t].s1 * coeff;
@@ -440,8 +524,8 @@ __global__ void __launch_bounds__(kSpineThreads) k_cv_finalize(FinalizeArgs a)
         rc->NN = a.N;
         rc->coeff_r = 1.0;
         rc->delta = __ddiv_rn(1.0, Nd);
+        rc->kbits = bin_kbits(a.N);
         rc->n_final = 0;
-        rc->ticket = 0;
         if (a.sys) {
             const uint64_t w = threefry_word(a.eng.key, a.eng.ctr, rc->offset);
             rc->u0 = __dmul_rn(canonical_u64(w), rc->delta);
@@ -453,7 +537,8 @@ __global__ void __launch_bounds__(kSpineThreads) k_cv_finalize(FinalizeArgs a)
 }
 
 // Monitor of a step that resampled and has no following move yet:
-// (1/N) sum_i x[copy_from[i]] (set_equal_weight then ISIntegrate).
+// (1/N) sum_i x[copy_from[i]] (set_equal_weight then ISIntegrate), plus the
+// anchor of the mixed form.
 template <typename Real>
 __global__ void __launch_bounds__(kThreads)
 k_cv_monitor_gather(const Real *x, const Real *y, const int32_t *copy_from,
@@ -487,6 +572,8 @@ k_cv_monitor_gather(const Real *x, const Real *y, const int32_t *copy_from,
 
 __global__ void k_cv_monitor_finish(const double *part, int nparts,
                                     long long N, long long t, FilterCtl *ctl,
+                                    const double *anchor_x,
+                                    const double *anchor_y,
                                     double *hist_mean_x, double *hist_mean_y)
 {
     if (threadIdx.x != 0)
@@ -496,12 +583,12 @@ __global__ void k_cv_monitor_finish(const double *part, int nparts,
         tx += part[2 * i];
         ty += part[2 * i + 1];
     }
-    hist_mean_x[t] = tx / (double)N;
-    hist_mean_y[t] = ty / (double)N;
+    hist_mean_x[t] = (anchor_x ? anchor_x[t] : 0.0) + tx / (double)N;
+    hist_mean_y[t] = (anchor_y ? anchor_y[t] : 0.0) + ty / (double)N;
     ctl->monitor_done = t;
 }
 
-// Gather of the final resampling into the current buffer (read_state).
+// Gather of the final resampling into the other buffer (read_state).
 template <typename Real>
 __global__ void k_gather_state(const Real *in, Real *out,
                                const int32_t *copy_from, long long N)
@@ -604,8 +691,9 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
     a.k0 = model_seed;
     a.k1 = 0;
     a.stream = c.stream_id;
-    a.p = CVParam{c.dt, c.sd_pos, c.sd_vel, c.sd_pos0, c.sd_vel0, c.scale,
-                  c.nu};
+    a.p = CVParam{c.dt,     c.sd_pos,     c.sd_vel,
+                  c.sd_pos0, c.sd_vel0,  c.scale,
+                  c.nu,     1.0 / c.nu, -0.5 * (c.nu + 1.0)};
     cudaEvent_t *ev = nullptr;
     if (f->timing) {
         if (f->ev_used + 3 > f->ev.size()) {
@@ -640,6 +728,9 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
     fa.threshold = c.threshold;
     fa.t = (long long)f->iter;
     fa.init = init ? 1 : 0;
+    fa.anchored = c.form == VSMC_CUDA_MIXED;
+    fa.obs_x = f->obs_x;
+    fa.obs_y = f->obs_y;
     fa.hist_ess = f->hist_ess;
     fa.hist_resampled = f->hist_resampled;
     fa.hist_logz_inc = f->hist_logz_inc;
@@ -650,7 +741,7 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
     fa.residual = residual;
     fa.sys = sys;
     fa.eng = f->eng;
-    k_cv_finalize<<<1, kSpineThreads, 0, s>>>(fa);
+    k_cv_finalize<<<1, kFinalThreads, 0, s>>>(fa);
 
     WeightsFromLog<Real> w;
     w.lw = static_cast<const Real *>(f->lw);
@@ -671,8 +762,10 @@ void launch_monitor_flush(vsmc_cuda_cv_filter *f)
         static_cast<const Real *>(f->state[f->cur][0]),
         static_cast<const Real *>(f->state[f->cur][1]), f->copy_from, N,
         f->mon_part);
+    const bool anch = f->cfg.form == VSMC_CUDA_MIXED;
     k_cv_monitor_finish<<<1, 32, 0, f->stream>>>(
         f->mon_part, kMonParts, N, (long long)f->iter - 1, f->ctl,
+        anch ? f->obs_x : nullptr, anch ? f->obs_y : nullptr,
         f->hist_mean_x, f->hist_mean_y);
 }
 
@@ -998,6 +1091,17 @@ int vsmc_cuda_cv_read_state(vsmc_cuda_cv_filter *f, double *x, double *y,
     if (e != cudaSuccess)
         return cuda_status(e, "read_state");
     double *outs[4] = {x, y, vx, vy};
+    // the mixed form stores positions as offsets from the last observation
+    double anchor[2] = {0.0, 0.0};
+    if (mixed && f->iter > 0) {
+        e = cudaMemcpy(&anchor[0], f->obs_x + (f->iter - 1), 8,
+                       cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(&anchor[1], f->obs_y + (f->iter - 1), 8,
+                           cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess)
+            return cuda_status(e, "read_state");
+    }
     // after a resampling the particles are the gathered previous ones
     const int src = f->cur, tmp = 1 - f->cur;
     for (int d = 0; d < 4; ++d) {
@@ -1025,8 +1129,9 @@ int vsmc_cuda_cv_read_state(vsmc_cuda_cv_filter *f, double *x, double *y,
             if (e == cudaSuccess)
                 e = cudaStreamSynchronize(f->stream);
             const float *fp = reinterpret_cast<const float *>(buf.data());
+            const double an = d < 2 ? anchor[d] : 0.0;
             for (size_t i = 0; i < N; ++i)
-                outs[d][i] = fp[i];
+                outs[d][i] = an + (double)fp[i];
         } else {
             e = cudaMemcpyAsync(outs[d], from, N * 8, cudaMemcpyDeviceToHost,
                                 f->stream);

@@ -34,13 +34,72 @@ struct ResampleCtl {
     long long n_final;    // uniforms consumed by particles 0..N-2
     unsigned long long words;   // engine words drawn by this call
     unsigned long long offset;  // engine offset before the call
-    unsigned long long ticket;  // dynamic tile counter of the invert kernel
+    int kbits;            // bin index: K = 2^kbits bins over [0, 1)
 };
 
 struct EngineRef {
     u64x4 key;
     u64x4 ctr;
 };
+
+// Bin index of a non-decreasing U01 sequence u_0..u_{NN-1}:
+// L[k] = #{n : u_n < k/K} for k = 0..K (K = 2^kbits, about NN/8), so the
+// count of u_n <= C for C in [k/K, (k+1)/K) lies in [L[k], L[k+1]].  Each
+// n writes the bins k with u_{n-1} < k/K <= u_n (k/K and u*K are exact), so
+// every bin is written exactly once; the owner of the last n also closes the
+// bins above u_{NN-1}.
+__device__ __forceinline__ int bin_kbits(long long NN)
+{
+    int kb = 0;
+    while (kb < 40 && (2ll << kb) <= NN / 8)
+        ++kb;
+    return kb;
+}
+
+__device__ __forceinline__ long long bin_floor(double u, int kb)
+{
+    // floor(u * K) clamped to [-1, K]
+    const double v = ldexp(u, kb);
+    const double K = ldexp(1.0, kb);
+    if (!(v >= 0.0))
+        return -1;
+    return v >= K ? (long long)K : (long long)v;
+}
+
+__device__ __forceinline__ void bin_write(int32_t *L, int kb, double uprev,
+                                          double u, long long n, long long NN)
+{
+    const long long K = 1ll << kb;
+    const long long klo = n == 0 ? 0 : bin_floor(uprev, kb) + 1;
+    long long khi = bin_floor(u, kb);
+    // k/K <= u  <=>  k <= floor(u K)
+    for (long long k = klo; k <= khi && k <= K; ++k)
+        L[k] = (int32_t)n;
+    if (n == NN - 1)
+        for (long long k = max(khi + 1, 0ll); k <= K; ++k)
+            L[k] = (int32_t)NN;
+}
+
+// Window of the count of u_n <= C from the bin index.
+__device__ __forceinline__ void bin_window(const int32_t *L, int kb,
+                                           long long NN, double C,
+                                           long long &lo, long long &hi)
+{
+    const long long K = 1ll << kb;
+    long long k = bin_floor(C, kb);
+    if (k < 0) {
+        lo = 0;
+        hi = L[0];
+        return;
+    }
+    if (k >= K) {
+        lo = L[K];
+        hi = NN;
+        return;
+    }
+    lo = L[k];
+    hi = L[k + 1];
+}
 
 // Weight sources --------------------------------------------------------
 // Normalised weights given in memory (generic C ABI).
@@ -224,8 +283,8 @@ k_spine_weights(const double *tile_sum, const long long *tile_k,
         ctl->NN = NN;
         ctl->coeff_r = coeff;
         ctl->delta = __ddiv_rn(1.0, (double)NN);
+        ctl->kbits = bin_kbits(NN);
         ctl->n_final = 0;
-        ctl->ticket = 0;
         if (Sys) {
             const uint64_t w = threefry_word(eng.key, eng.ctr, ctl->offset);
             ctl->u0 = __dmul_rn(canonical_u64(w), ctl->delta);
@@ -236,50 +295,118 @@ k_spine_weights(const double *tile_sum, const long long *tile_k,
     }
 }
 
+// Words at stream positions pos0 .. pos0+7 of a Threefry4x64 engine (two or
+// three block evaluations).
+__device__ __forceinline__ void threefry_words8(const EngineRef &eng,
+                                                unsigned long long pos0,
+                                                uint64_t w[8])
+{
+    const unsigned long long b0 = pos0 / 4;
+    const int s = (int)(pos0 % 4);
+    const u64x4 x = threefry4x64_20(ctr64_add(eng.ctr, b0 + 1), eng.key);
+    const u64x4 y = threefry4x64_20(ctr64_add(eng.ctr, b0 + 2), eng.key);
+    u64x4 z;
+    z.v[0] = z.v[1] = z.v[2] = z.v[3] = 0;
+    if (s > 0)
+        z = threefry4x64_20(ctr64_add(eng.ctr, b0 + 3), eng.key);
+    const uint64_t q[12] = {x.v[0], x.v[1], x.v[2], x.v[3], y.v[0], y.v[1],
+                            y.v[2], y.v[3], z.v[0], z.v[1], z.v[2], z.v[3]};
+    // w[j] = q[s + j] with constant indices only (register selects)
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        w[j] = s == 0 ? q[j] : s == 1 ? q[j + 1] : s == 2 ? q[j + 2] : q[j + 3];
+}
+
 // Stratified U01 sequence (U01SequenceStratified, u01.hpp:212-243):
-// u_n = U_n * delta + n * delta, U_n from engine word offset + n.  Adjacent
-// values can cross by rounding only between neighbours, so the running
-// maximum is max(u_n, u_{n-1}).
+// u_n = U_n * delta + n * delta, U_n from engine word offset + n.  One
+// Threefry block per thread gives four consecutive u_n.  Adjacent values can
+// cross by rounding only between neighbours, so the running maximum is
+// max(u_n, u_{n-1}); the neighbour of a thread's first value comes from the
+// previous lane (lane 0 recomputes it).
+__device__ __forceinline__ double strat_u(uint64_t w, long long n, double delta)
+{
+    return __dadd_rn(__dmul_rn(canonical_u64(w), delta),
+                     __dmul_rn((double)n, delta));
+}
+
 static __global__ void __launch_bounds__(kThreads)
-k_uniforms_stratified(EngineRef eng, const ResampleCtl *ctl, double *u)
+k_uniforms_stratified(EngineRef eng, const ResampleCtl *ctl, double *u,
+                      int32_t *L)
 {
     if (!ctl->active)
         return;
     const long long NN = ctl->NN;
     const double delta = ctl->delta;
+    const int kb = ctl->kbits;
     const unsigned long long off = ctl->offset;
-    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= NN)
-        return;
-    const double a = __dadd_rn(
-        __dmul_rn(canonical_u64(threefry_word(eng.key, eng.ctr, off + n)),
-                  delta),
-        __dmul_rn((double)n, delta));
-    double v = a;
-    if (n > 0) {
-        const double p = __dadd_rn(
-            __dmul_rn(canonical_u64(threefry_word(eng.key, eng.ctr,
-                                                  off + n - 1)),
-                      delta),
-            __dmul_rn((double)(n - 1), delta));
-        v = fmax(a, p);
+    const unsigned long long b =
+        off / 4 + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = b * 4 < off + (unsigned long long)NN;
+    double raw[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    if (live) {
+        const u64x4 w = threefry4x64_20(ctr64_add(eng.ctr, b + 1), eng.key);
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            const long long n = (long long)(b * 4 + l) - (long long)off;
+            if (n >= 0 && n < NN)
+                raw[l] = strat_u(w.v[l], n, delta);
+        }
     }
-    u[n] = v;
+    // raw values of n-1 and n-2 for the thread's first n
+    double p1 = __shfl_up_sync(0xffffffffu, raw[3], 1);
+    double p2 = __shfl_up_sync(0xffffffffu, raw[2], 1);
+    if ((threadIdx.x & 31) == 0) {
+        p1 = p2 = -INFINITY;
+        const long long n = (long long)(b * 4) - (long long)off;
+        if (live && n - 1 >= 0 && n - 1 < NN)
+            p1 = strat_u(threefry_word(eng.key, eng.ctr, off + n - 1), n - 1,
+                         delta);
+        if (live && n - 2 >= 0 && n - 2 < NN)
+            p2 = strat_u(threefry_word(eng.key, eng.ctr, off + n - 2), n - 2,
+                         delta);
+    }
+    if (!live)
+        return;
+    // monotone sequence v_n = max(u_n, u_{n-1}); vprev = v_{n-1}
+    double vprev = fmax(p1, p2), rprev = p1;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        const long long n = (long long)(b * 4 + l) - (long long)off;
+        if (n >= 0 && n < NN) {
+            const double v = fmax(raw[l], rprev);
+            u[n] = v;
+            bin_write(L, kb, vprev, v, n, NN);
+            vprev = v;
+        }
+        rprev = raw[l];
+    }
 }
 
 // Sorted U01 sequence (U01SequenceSorted, u01.hpp:165-202): lmax_n =
 // sum_{k<=n} log(1 - U_k) / (NN - k); u_n = 1 - exp(lmax_n).  Two passes
-// over tiles of kTile uniforms around a deterministic spine.
-__device__ __forceinline__ double sorted_term(const EngineRef &eng,
+// over tiles of kTile uniforms around a deterministic spine; each thread owns
+// 8 consecutive n.
+__device__ __forceinline__ void sorted_terms8(const EngineRef &eng,
                                               unsigned long long off,
-                                              long long n, long long NN)
+                                              long long n0, long long NN,
+                                              double t[8])
 {
-    const double U = canonical_u64(threefry_word(eng.key, eng.ctr, off + n));
-    return __ddiv_rn(log(__dadd_rn(1.0, -U)), (double)(NN - n));
+    uint64_t w[8];
+    threefry_words8(eng, off + (unsigned long long)n0, w);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const long long n = n0 + j;
+        const double U = canonical_u64(w[j]);
+        t[j] = n < NN ? __ddiv_rn(log(__dadd_rn(1.0, -U)), (double)(NN - n))
+                      : 0.0;
+    }
 }
 
+// Pass 1: the terms log(1 - U_n) / (NN - n), stored in u[] for pass 2,
+// and their tile sums.
 static __global__ void __launch_bounds__(kThreads)
-k_sorted_tile_sums(EngineRef eng, const ResampleCtl *ctl, double *tile_sum)
+k_sorted_tile_sums(EngineRef eng, const ResampleCtl *ctl, double *tile_sum,
+                   double *u)
 {
     if (!ctl->active)
         return;
@@ -288,11 +415,15 @@ k_sorted_tile_sums(EngineRef eng, const ResampleCtl *ctl, double *tile_sum)
     const long long base = (long long)blockIdx.x * kTile;
     if (base >= NN)
         return;
+    double t[kItems];
+    const long long n0 = base + (long long)threadIdx.x * kItems;
+    sorted_terms8(eng, ctl->offset, n0, NN, t);
     double s = 0.0;
+#pragma unroll
     for (int j = 0; j < kItems; ++j) {
-        const long long n = base + (long long)threadIdx.x * kItems + j;
-        if (n < NN)
-            s += sorted_term(eng, ctl->offset, n, NN);
+        s += t[j];
+        if (n0 + j < NN)
+            u[n0 + j] = t[j];
     }
     double total;
     block_excl_scan(s, sh, total);
@@ -313,47 +444,44 @@ k_sorted_spine(const double *tile_sum, double *tile_excl,
 
 static __global__ void __launch_bounds__(kThreads)
 k_sorted_uniforms(EngineRef eng, const ResampleCtl *ctl,
-                  const double *tile_excl, double *u)
+                  const double *tile_excl, double *u, int32_t *L)
 {
     if (!ctl->active)
         return;
     __shared__ double sh[kThreads / 32];
+    __shared__ double shm[kThreads];
     const long long NN = ctl->NN;
     const long long base = (long long)blockIdx.x * kTile;
     if (base >= NN)
         return;
     const long long last = min(base + (long long)kTile, NN) - 1;
     double t[kItems];
+    const long long n0 = base + (long long)threadIdx.x * kItems;
+#pragma unroll
+    for (int j = 0; j < kItems; ++j)
+        t[j] = n0 + j < NN ? u[n0 + j] : 0.0; // pass 1 stored the terms
     double run = 0.0;
 #pragma unroll
-    for (int j = 0; j < kItems; ++j) {
-        const long long n = base + (long long)threadIdx.x * kItems + j;
-        t[j] = n < NN ? sorted_term(eng, ctl->offset, n, NN) : 0.0;
+    for (int j = 0; j < kItems; ++j)
         run += t[j];
-    }
     double total;
     double pre = block_excl_scan(run, sh, total);
     const double a = tile_excl[blockIdx.x];
     const double b = tile_excl[blockIdx.x + 1];
     // carry: the previous tile ends exactly at lmax = a
-    double umax = blockIdx.x > 0 ? __dadd_rn(1.0, -exp(a)) : -INFINITY;
+    const double umax = blockIdx.x > 0 ? __dadd_rn(1.0, -exp(a)) : -INFINITY;
     double uv[kItems];
-#pragma unroll
-    for (int j = 0; j < kItems; ++j) {
-        const long long n = base + (long long)threadIdx.x * kItems + j;
-        pre += t[j];
-        double lmax = fmax(__dadd_rn(a, pre), b); // lmax is non-increasing
-        if (n == last)
-            lmax = b;
-        uv[j] = __dadd_rn(1.0, -exp(lmax));
-    }
-    // running max within the thread, then across the block
     double tmax = -INFINITY;
 #pragma unroll
-    for (int j = 0; j < kItems; ++j)
+    for (int j = 0; j < kItems; ++j) {
+        pre += t[j];
+        double lmax = fmax(__dadd_rn(a, pre), b); // lmax is non-increasing
+        if (n0 + j == last)
+            lmax = b;
+        uv[j] = __dadd_rn(1.0, -exp(lmax));
         tmax = fmax(tmax, uv[j]);
-    // block exclusive max-scan via shared memory
-    __shared__ double shm[kThreads];
+    }
+    // block exclusive max-scan
     shm[threadIdx.x] = tmax;
     __syncthreads();
     for (int o = 1; o < kThreads; o <<= 1) {
@@ -364,18 +492,34 @@ k_sorted_uniforms(EngineRef eng, const ResampleCtl *ctl,
         __syncthreads();
     }
     double m = threadIdx.x > 0 ? fmax(umax, shm[threadIdx.x - 1]) : umax;
+    const int kb = ctl->kbits;
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-        const long long n = base + (long long)threadIdx.x * kItems + j;
+        const double prevm = m;
         m = fmax(m, uv[j]);
-        if (n < NN)
-            u[n] = m;
+        if (n0 + j < NN) {
+            u[n0 + j] = m;
+            bin_write(L, kb, prevm, m, n0 + j, NN);
+        }
     }
 }
 
 // ---------------------------------------------------------------------------
 // Count of the U01 sequence values <= C ("first n with u_n > C", which for a
 // non-decreasing sequence is the upper bound).
+__device__ __forceinline__ int ub_shared(const double *u, int lo, int hi,
+                                         double C)
+{
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (u[mid] <= C)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
 __device__ __forceinline__ long long ub_global(const double *u, long long lo,
                                                long long hi, double C)
 {
@@ -389,17 +533,29 @@ __device__ __forceinline__ long long ub_global(const double *u, long long lo,
     return lo;
 }
 
-__device__ __forceinline__ int ub_shared(const double *u, int lo, int hi,
-                                         double C)
+// Warp-cooperative upper bound over a non-decreasing sequence f(0..n-1):
+// each round the 32 lanes probe 32 evenly spaced points, so a range of n
+// shrinks by 33x per global-memory round trip.  Every lane returns the
+// count of indices with f(i) <= C.
+template <typename F>
+__device__ __forceinline__ long long warp_upper_bound(F f, long long lo,
+                                                      long long hi, double C)
 {
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (u[mid] <= C)
-            lo = mid + 1;
-        else
-            hi = mid;
+    const int lane = threadIdx.x & 31;
+    while (hi - lo > 32) {
+        const long long span = hi - lo;
+        const long long p = lo + (span * (lane + 1)) / 33;
+        const unsigned le = __ballot_sync(0xffffffffu, f(p) <= C);
+        const int k = __popc(le); // probes are increasing: a prefix is true
+        const long long nlo =
+            k > 0 ? lo + (span * k) / 33 + 1 : lo;
+        const long long nhi = k < 32 ? lo + (span * (k + 1)) / 33 : hi;
+        lo = nlo;
+        hi = nhi;
     }
-    return lo;
+    const long long p = lo + lane;
+    const bool le = p < hi && f(p) <= C;
+    return lo + __popc(__ballot_sync(0xffffffffu, le));
 }
 
 // Systematic (U01SequenceSystematic, u01.hpp:253-287): u_n = u0 + n delta,
@@ -430,59 +586,33 @@ __device__ __forceinline__ long long sys_count(double C, double u0,
     return n;
 }
 
-constexpr int kUStage = kTile; // uniforms staged in shared memory per tile (the
-                                // weight buffer is reused, kTile doubles)
-constexpr unsigned long long kSpinLimit = 1ull << 22;
+constexpr int kUStage = kTile; // uniforms staged in shared memory per tile
 
-// Look-back status word: bits 62-63 flag (1 aggregate, 2 inclusive prefix),
-// low 32 bits the zero-slot count.
-__device__ __forceinline__ void lb_publish(unsigned long long *st, int flag,
-                                           unsigned count)
-{
-    const unsigned long long v =
-        ((unsigned long long)flag << 62) | (unsigned long long)count;
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(st), "l"(v)
-                 : "memory");
-}
-
-__device__ __forceinline__ unsigned long long lb_load(
-    const unsigned long long *st)
-{
-    unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];"
-                 : "=l"(v)
-                 : "l"(st)
-                 : "memory");
-    return v;
-}
-
-// The inversion + cfrp ranks kernel.  Residual: weights are r * coeff_r and
-// k = floor(N w) is added back (residual.hpp:59-76).  Sys: closed-form
-// count.  Outputs: replication (optional), copy_from (self for survivors,
-// -(rank+1) for the rank-th zero slot) and sinc (inclusive count of surplus
-// children, sum_{j<=i} max(rep_j - 1, 0)).
+// The inversion kernel (internal::inversion, common.hpp:57-84, on the FP64
+// scan of the weights) and the first half of internal::cfrp_trans.
+// Residual: weights are r * coeff_r and k = floor(N w) is added back
+// (residual.hpp:59-76).  Sys: closed-form count.  Outputs: replication
+// (optional), copy_from (self for survivors, -(r+1) for the tile's r-th
+// slot without offspring), sinc_local (surplus children of particles <= i
+// minus the zero slots of earlier tiles) and the tile's zero-slot count.
 template <typename W, bool Residual, bool Sys>
 __global__ void __launch_bounds__(kThreads)
 k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
          const long long *tile_kexcl, const double *u, long long n_u,
-         unsigned long long *lb_status, int32_t *rep_out, int32_t *copy_from,
-         int32_t *sinc)
+         const int32_t *L, int32_t *rep_out, int32_t *copy_from,
+         int32_t *sinc_local, int32_t *tile_zeros, int32_t *tile_sinc_last)
 {
     if (!ctl->active)
         return;
-    __shared__ double sw[kTile];         // weights, then staged uniforms
+    __shared__ double sw[kTile];                // weights, then uniforms
     __shared__ double sk[Residual ? kTile : 1]; // floor(N w) (residual)
     __shared__ long long shl[kThreads / 32];
     __shared__ double shd[kThreads / 32];
     __shared__ long long sh_bound[2];
-    __shared__ unsigned sh_zexcl;
-    __shared__ unsigned sh_tile;
+    __shared__ long long sh_last[kThreads / 32];
     wsrc.prepare();
 
-    if (threadIdx.x == 0)
-        sh_tile = (unsigned)atomicAdd(&ctl->ticket, 1ull);
-    __syncthreads();
-    const int tile = (int)sh_tile;
+    const int tile = blockIdx.x;
     const long long base = (long long)tile * kTile;
     const long long NN = ctl->NN;
     const double Nd = (double)N;
@@ -490,7 +620,29 @@ k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     const double u0 = Sys ? ctl->u0 : 0.0;
     const double delta = ctl->delta;
     const long long nu = Sys ? NN : min(NN, n_u);
+    const double a = tile_excl[tile];
+    const double b = tile_excl[tile + 1];
 
+    // uniforms that can fall in this tile: (ub(a), ub(b)], each found in a
+    // bin window of about 8 values by one warp while the others load weights
+    const int wid = threadIdx.x >> 5;
+    if (wid < 2) {
+        const double C = wid == 0 ? a : b;
+        long long r;
+        if (wid == 0 && tile == 0) {
+            r = 0;
+        } else if (Sys) {
+            r = sys_count(C, u0, delta, NN);
+        } else {
+            long long wl, wh;
+            bin_window(L, ctl->kbits, nu, C, wl, wh);
+            wl = min(wl, nu);
+            wh = min(max(wh, wl), nu);
+            r = warp_upper_bound([u](long long i) { return u[i]; }, wl, wh, C);
+        }
+        if ((threadIdx.x & 31) == 0)
+            sh_bound[wid] = r;
+    }
     // striped (coalesced) load of the tile's weights into shared memory
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
@@ -515,28 +667,13 @@ k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
         run += wv[j];
     }
     double total;
-    double pre = block_excl_scan(run, shd, total);
-    const double a = tile_excl[tile];
-    const double b = tile_excl[tile + 1];
-
-    // uniforms that can fall in this tile: (ub(a), ub(b)]
-    if (threadIdx.x == 0) {
-        if (Sys) {
-            sh_bound[0] = tile > 0 ? sys_count(a, u0, delta, NN) : 0;
-            sh_bound[1] = sys_count(b, u0, delta, NN);
-        } else {
-            sh_bound[0] = tile > 0 ? ub_global(u, 0, nu, a) : 0;
-            sh_bound[1] = ub_global(u, sh_bound[0], nu, b);
-        }
-    }
-    __syncthreads(); // also: every thread has read sw
+    double pre = block_excl_scan(run, shd, total); // ends with a barrier
     const long long lo = sh_bound[0];
     const long long hi = max(sh_bound[1], lo);
     const bool staged = !Sys && (hi - lo) <= kUStage;
-    if (staged) {
+    if (staged)
         for (long long n = lo + threadIdx.x; n < hi; n += kThreads)
             sw[n - lo] = u[n];
-    }
     __syncthreads();
 
     // counts c_i = #{n: u_n <= C_i} for this thread's particles
@@ -562,22 +699,17 @@ k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
         cnt[j] = min(max(c, lo), i >= N - 1 ? NN : hi);
         k_int[j] = Residual ? (long long)sk[threadIdx.x * kItems + j] : 0;
     }
-    // non-decreasing counts within the thread; neighbour's last count
 #pragma unroll
     for (int j = 1; j < kItems; ++j)
         cnt[j] = max(cnt[j], cnt[j - 1]);
     long long prev = __shfl_up_sync(0xffffffffu, cnt[kItems - 1], 1);
-    __shared__ long long sh_last[kThreads / 32];
     if ((threadIdx.x & 31) == 31)
-        sh_last[threadIdx.x >> 5] = cnt[kItems - 1];
+        sh_last[wid] = cnt[kItems - 1];
     __syncthreads();
     if ((threadIdx.x & 31) == 0)
-        prev = (threadIdx.x == 0) ? (tile > 0 ? lo : 0)
-                                  : sh_last[(threadIdx.x >> 5) - 1];
-    // warp-level running max of prev across threads is implied by the
-    // per-thread clamps to [lo, hi] and the monotone C_i.
+        prev = (threadIdx.x == 0) ? (tile > 0 ? lo : 0) : sh_last[wid - 1];
     long long rep[kItems];
-    unsigned zeros = 0;
+    int zeros = 0;
     long long ksum = 0;
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
@@ -586,7 +718,7 @@ k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
         rep[j] = (i < N) ? (c - prev) + k_int[j] : 0;
         prev = c;
         cnt[j] = c;
-        zeros += (i < N && rep[j] == 0) ? 1u : 0u;
+        zeros += (i < N && rep[j] == 0) ? 1 : 0;
         ksum += k_int[j];
     }
     // the last queried uniform fixes the words drawn (inversion queries
@@ -601,47 +733,14 @@ k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
                                       : 0ull;
         }
     }
-
-    // zero-slot counts: block scan, then the tile look-back
     long long ztot;
-    const long long zex_thread = block_excl_scan((long long)zeros, shl, ztot);
+    long long zloc = block_excl_scan((long long)zeros, shl, ztot);
     long long ktot;
-    const long long kex_thread = Residual ? block_excl_scan(ksum, shl, ktot)
-                                          : 0;
-    if (threadIdx.x == 0) {
-        unsigned long long *st = lb_status + tile;
-        if (tile == 0) {
-            lb_publish(st, 2, (unsigned)ztot);
-            sh_zexcl = 0;
-        } else {
-            lb_publish(st, 1, (unsigned)ztot);
-            unsigned excl = 0;
-            int p = tile - 1;
-            unsigned long long spins = 0;
-            while (p >= 0) {
-                const unsigned long long v = lb_load(lb_status + p);
-                const int flag = (int)(v >> 62);
-                if (flag == 0) {
-                    if (++spins > kSpinLimit) {
-                        atomicExch(&ctl->error, (int)VSMC_CUDA_ETIMEOUT);
-                        break;
-                    }
-                    __nanosleep(32);
-                    continue;
-                }
-                excl += (unsigned)(v & 0xffffffffull);
-                if (flag == 2)
-                    break;
-                --p;
-            }
-            lb_publish(st, 2, excl + (unsigned)ztot);
-            sh_zexcl = excl;
-        }
-    }
-    __syncthreads();
-    long long zeros_before = (long long)sh_zexcl + zex_thread;
-    const long long kbase = Residual ? tile_kexcl[tile] + kex_thread : 0;
-    long long kprefix = kbase;
+    const long long kex = Residual ? block_excl_scan(ksum, shl, ktot) : 0;
+    if (threadIdx.x == 0)
+        tile_zeros[tile] = (int32_t)ztot;
+    const long long tile_last = min(base + (long long)kTile, N) - 1;
+    long long kprefix = Residual ? tile_kexcl[tile] + kex : 0;
     int32_t cf[kItems], sc[kItems], rp[kItems];
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
@@ -650,37 +749,32 @@ k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
         // R_{<=i} = count_i + K_{<=i}; the last particle closes at N
         const long long R = (i >= N - 1) ? N : cnt[j] + kprefix;
         if (rep[j] == 0) {
-            cf[j] = (int32_t)(-(zeros_before + 1));
-            ++zeros_before;
+            cf[j] = (int32_t)(-(zloc + 1));
+            ++zloc;
         } else {
             cf[j] = (int32_t)i;
         }
-        sc[j] = (int32_t)(R - (i + 1) + zeros_before);
+        sc[j] = (int32_t)(R - (i + 1) + zloc);
         rp[j] = (int32_t)rep[j];
+        if (i == tile_last)
+            tile_sinc_last[tile] = sc[j];
     }
-    // stage the three outputs through shared memory for coalesced stores
+    // stage the outputs through shared memory for coalesced stores
     __syncthreads();
     int32_t *s32 = reinterpret_cast<int32_t *>(sw);
 #pragma unroll
-    for (int j = 0; j < kItems; ++j)
-        s32[threadIdx.x * kItems + j] = cf[j];
-    __syncthreads();
-#pragma unroll
     for (int j = 0; j < kItems; ++j) {
-        const long long i = base + (long long)j * kThreads + threadIdx.x;
-        if (i < N)
-            copy_from[i] = s32[j * kThreads + threadIdx.x];
+        s32[threadIdx.x * kItems + j] = cf[j];
+        s32[kTile + threadIdx.x * kItems + j] = sc[j];
     }
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < kItems; ++j)
-        s32[threadIdx.x * kItems + j] = sc[j];
-    __syncthreads();
-#pragma unroll
     for (int j = 0; j < kItems; ++j) {
         const long long i = base + (long long)j * kThreads + threadIdx.x;
-        if (i < N)
-            sinc[i] = s32[j * kThreads + threadIdx.x];
+        if (i < N) {
+            copy_from[i] = s32[j * kThreads + threadIdx.x];
+            sinc_local[i] = s32[kTile + j * kThreads + threadIdx.x];
+        }
     }
     if (rep_out != nullptr) {
         __syncthreads();
@@ -697,65 +791,135 @@ k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     }
 }
 
-// Parent of the rank-th surplus child: the first p with sinc[p] > rank,
-// found by galloping outwards from the zero slot's own index.
-__device__ __forceinline__ int32_t cfrp_parent(const int32_t *sinc,
-                                               long long N, long long i,
-                                               long long rank)
+// Exclusive prefix of the per-tile zero-slot counts (one CTA) and, per
+// tile, the range of tiles holding the parents of its zero slots.  The
+// surplus count at the end of tile t is E[t] = tile_sinc_last[t] + zexcl[t]
+// (non-decreasing); the parent of rank k is in the first tile with
+// E > k, found by a binary search over E staged in shared memory.
+constexpr int kSpineStage = 8192; // tiles whose E fits in shared memory
+
+static __global__ void __launch_bounds__(kSpineThreads)
+k_zero_spine(const int32_t *tile_zeros, const int32_t *tile_sinc_last,
+             int32_t *zexcl, int32_t *tfirst, int32_t *tlast, int ntiles,
+             const ResampleCtl *ctl)
 {
-    long long lo, hi; // invariant: sinc[lo] <= rank < sinc[hi] (virtual ends)
-    if (sinc[i] > rank) {
-        hi = i;
-        long long step = 1;
-        lo = i - 1;
-        while (lo >= 0 && sinc[lo] > rank) {
-            hi = lo;
-            lo = i - (step <<= 1);
-        }
-        if (lo < -1)
-            lo = -1;
-    } else {
-        lo = i;
-        long long step = 1;
-        hi = i + 1;
-        while (hi < N && sinc[hi] <= rank) {
-            lo = hi;
-            hi = i + (step <<= 1);
-        }
-        if (hi > N)
-            hi = N;
+    if (!ctl->active)
+        return;
+    __shared__ long long sh[kSpineThreads / 32];
+    __shared__ int32_t E[kSpineStage];
+    const int per = (ntiles + blockDim.x - 1) / blockDim.x;
+    const int b = threadIdx.x * per;
+    const int e = min(b + per, ntiles);
+    long long run = 0;
+    for (int t = b; t < e; ++t)
+        run += tile_zeros[t];
+    long long total;
+    run = block_excl_scan(run, sh, total);
+    for (int t = b; t < e; ++t) {
+        zexcl[t] = (int32_t)run;
+        if (t < kSpineStage)
+            E[t] = (int32_t)(tile_sinc_last[t] + run);
+        run += tile_zeros[t];
     }
-    while (hi - lo > 1) {
-        const long long mid = lo + ((hi - lo) >> 1);
-        if (sinc[mid] > rank)
-            hi = mid;
-        else
-            lo = mid;
+    if (threadIdx.x == blockDim.x - 1)
+        zexcl[ntiles] = (int32_t)total;
+    __syncthreads();
+    const bool staged = ntiles <= kSpineStage;
+    auto Eat = [&](int t) {
+        return staged ? (long long)E[t]
+                      : (long long)tile_sinc_last[t] + zexcl[t];
+    };
+    auto first_tile_above = [&](long long k) {
+        int lo = 0, hi = ntiles - 1;
+        while (lo < hi) {
+            const int m = (lo + hi) >> 1;
+            if (Eat(m) > k)
+                hi = m;
+            else
+                lo = m + 1;
+        }
+        return lo;
+    };
+    for (int t = threadIdx.x; t < ntiles; t += blockDim.x) {
+        const long long z0 = zexcl[t];
+        const long long z1 = t + 1 < ntiles ? (long long)zexcl[t + 1] : total;
+        if (z0 == z1) {
+            tfirst[t] = 0;
+            tlast[t] = -1;
+        } else {
+            tfirst[t] = first_tile_above(z0);
+            tlast[t] = first_tile_above(z1 - 1);
+        }
     }
-    return (int32_t)hi; // N when no parent exists (caller checks)
 }
 
-// internal::cfrp_trans for the zero slots (common.hpp:94-106): the k-th
-// slot without offspring takes the k-th surplus child in parent order.
+// internal::cfrp_trans for the slots without offspring (common.hpp:94-106):
+// the k-th such slot takes the k-th surplus child in parent order, i.e. the
+// first parent p with sinc(p) > k, sinc(p) = sinc_local[p] + zexcl[tile(p)].
+// The CTA of tile t stages the parent tiles tfirst[t]..tlast[t] one at a
+// time in shared memory; every slot binary-searches its parent there.
 static __global__ void __launch_bounds__(kThreads)
-k_cfrp_fill(long long N, const ResampleCtl *ctl, const int32_t *sinc,
+k_cfrp_fill(long long N, ResampleCtl *ctl, const int32_t *sinc_local,
+            const int32_t *zexcl, const int32_t *tfirst, const int32_t *tlast,
             int32_t *copy_from)
 {
     if (!ctl->active)
         return;
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N)
-        return;
-    const int32_t c = copy_from[i];
-    if (c >= 0)
-        return;
-    const int32_t p = cfrp_parent(sinc, N, i, (long long)(-c) - 1);
-    if (p >= N) { // replication did not sum to N: never index past the end
-        atomicExch(const_cast<int *>(&ctl->error), (int)VSMC_CUDA_EDEGENERATE);
-        copy_from[i] = (int32_t)i;
-        return;
+    __shared__ int32_t ss[kTile];
+    const int tile = blockIdx.x;
+    const int t0 = tfirst[tile], t1 = tlast[tile];
+    if (t1 < t0)
+        return; // every particle of the tile has offspring
+    const long long Z0 = zexcl[tile];
+    const long long base = (long long)tile * kTile;
+    long long rank[kItems];
+    int32_t parent[kItems];
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        const long long i = base + (long long)j * kThreads + threadIdx.x;
+        rank[j] = -1;
+        parent[j] = 0;
+        if (i < N) {
+            const int32_t c = copy_from[i];
+            if (c < 0)
+                rank[j] = Z0 + (long long)(-c) - 1;
+        }
     }
-    copy_from[i] = p;
+    for (int pt = t0; pt <= t1; ++pt) {
+        const long long pb = (long long)pt * kTile;
+        const int len = (int)min((long long)kTile, N - pb);
+        const int32_t zoff = zexcl[pt];
+        for (int j = threadIdx.x; j < len; j += kThreads)
+            ss[j] = sinc_local[pb + j] + zoff;
+        __syncthreads();
+        const long long top = ss[len - 1];
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) {
+            if (rank[j] >= 0 && rank[j] < top) {
+                int l = 0, h = len - 1; // first index with ss > rank
+                while (l < h) {
+                    const int m = (l + h) >> 1;
+                    if (ss[m] > rank[j])
+                        h = m;
+                    else
+                        l = m + 1;
+                }
+                parent[j] = (int32_t)(pb + l);
+                rank[j] = -2;
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        const long long i = base + (long long)j * kThreads + threadIdx.x;
+        if (rank[j] == -2) {
+            copy_from[i] = parent[j];
+        } else if (rank[j] >= 0) { // no parent found: replication != N
+            atomicExch(&ctl->error, (int)VSMC_CUDA_EDEGENERATE);
+            copy_from[i] = (int32_t)i;
+        }
+    }
 }
 
 // Finalise the engine position.
@@ -767,7 +931,7 @@ static __global__ void k_resample_done(ResampleCtl *ctl)
 }
 
 // Running maximum of caller-supplied uniforms (parity mode): tile maxima,
-// spine, apply.
+// then each tile folds the maxima before it.
 static __global__ void __launch_bounds__(kThreads)
 k_tile_max(const double *u, long long n, double *tile_max)
 {
@@ -792,7 +956,8 @@ k_tile_max(const double *u, long long n, double *tile_max)
 }
 
 static __global__ void __launch_bounds__(kThreads)
-k_apply_max(const double *u, long long n, const double *tile_max, double *out)
+k_apply_max(const double *u, long long n, const double *tile_max, double *out,
+            const ResampleCtl *ctl, int32_t *L)
 {
     __shared__ double carry_sh;
     __shared__ double shm[kThreads];
@@ -821,26 +986,35 @@ k_apply_max(const double *u, long long n, const double *tile_max, double *out)
     }
     double m = fmax(carry_sh, threadIdx.x > 0 ? shm[threadIdx.x - 1]
                                               : -INFINITY);
+    const int kb = ctl->kbits;
     for (int j = 0; j < kItems; ++j) {
         const long long i = base + (long long)threadIdx.x * kItems + j;
+        const double prevm = m;
         m = fmax(m, v[j]);
-        if (i < n)
+        if (i < n) {
             out[i] = m;
+            bin_write(L, kb, prevm, m, i, n);
+        }
     }
 }
 
 // ------------------------------------------------------------ host side --
 struct ResampleWorkspace {
     ResampleCtl *ctl;
-    double *tile_sum;     // ntiles + 1
-    double *tile_excl;    // ntiles + 1
-    long long *tile_k;    // ntiles + 1
+    double *tile_sum;      // ntiles + 1
+    double *tile_excl;     // ntiles + 1
+    long long *tile_k;     // ntiles + 1
     long long *tile_kexcl; // ntiles + 1
-    double *u;            // N
-    double *u_tile_sum;   // ntiles + 1
-    double *u_tile_excl;  // ntiles + 1
-    unsigned long long *lb_status; // ntiles
-    int32_t *sinc;        // N
+    double *u_tile_sum;    // ntiles + 1
+    double *u_tile_excl;   // ntiles + 1
+    int32_t *tile_zeros;   // ntiles + 1
+    int32_t *zexcl;        // ntiles + 1
+    int32_t *tile_sinc_last; // ntiles + 1
+    int32_t *tfirst;       // ntiles + 1
+    int32_t *tlast;        // ntiles + 1
+    int32_t *bins;         // N / 8 + 2 (bin index of the U01 sequence)
+    double *u;             // N
+    int32_t *sinc;         // N (tile-local surplus counts)
 };
 
 inline int resample_ntiles(long long N)
@@ -854,8 +1028,8 @@ inline size_t resample_workspace_bytes(long long N)
 {
     const size_t nt = (size_t)resample_ntiles(N) + 1;
     return align256(sizeof(ResampleCtl)) + 6 * align256(nt * 8) +
-           align256(nt * 8) /* lb */ + align256((size_t)N * 8) +
-           align256((size_t)N * 4);
+           5 * align256(nt * 4) + align256(((size_t)N / 8 + 2) * 4) +
+           align256((size_t)N * 8) + align256((size_t)N * 4);
 }
 
 inline ResampleWorkspace carve_workspace(void *base, long long N)
@@ -877,8 +1051,18 @@ inline ResampleWorkspace carve_workspace(void *base, long long N)
     p += align256(nt * 8);
     w.u_tile_excl = reinterpret_cast<double *>(p);
     p += align256(nt * 8);
-    w.lb_status = reinterpret_cast<unsigned long long *>(p);
-    p += align256(nt * 8);
+    w.tile_zeros = reinterpret_cast<int32_t *>(p);
+    p += align256(nt * 4);
+    w.zexcl = reinterpret_cast<int32_t *>(p);
+    p += align256(nt * 4);
+    w.tile_sinc_last = reinterpret_cast<int32_t *>(p);
+    p += align256(nt * 4);
+    w.tfirst = reinterpret_cast<int32_t *>(p);
+    p += align256(nt * 4);
+    w.tlast = reinterpret_cast<int32_t *>(p);
+    p += align256(nt * 4);
+    w.bins = reinterpret_cast<int32_t *>(p);
+    p += align256(((size_t)N / 8 + 2) * 4);
     w.u = reinterpret_cast<double *>(p);
     p += align256((size_t)N * 8);
     w.sinc = reinterpret_cast<int32_t *>(p);
@@ -895,7 +1079,7 @@ inline int resample_launches(int scheme, bool parity)
                      scheme == VSMC_CUDA_RESIDUAL_SYSTEMATIC;
     const bool strat = scheme == VSMC_CUDA_STRATIFIED ||
                        scheme == VSMC_CUDA_RESIDUAL_STRATIFIED;
-    int n = 3; // invert, cfrp fill, done
+    int n = 4; // invert, zero spine, cfrp fill, done
     if (residual)
         n += 2;
     if (parity)
@@ -956,26 +1140,29 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
             k_tile_max<<<ntu, kThreads, 0, s>>>(u_given, n_given,
                                                 ws.u_tile_sum);
             k_apply_max<<<ntu, kThreads, 0, s>>>(u_given, n_given,
-                                                 ws.u_tile_sum, ws.u);
+                                                 ws.u_tile_sum, ws.u, ws.ctl,
+                                                 ws.bins);
         }
         n_u = n_given;
     } else if (strat) {
-        k_uniforms_stratified<<<(unsigned)((N + kThreads - 1) / kThreads),
-                                kThreads, 0, s>>>(eng, ws.ctl, ws.u);
+        const long long blocks = N / 4 + 2;
+        k_uniforms_stratified<<<(unsigned)((blocks + kThreads - 1) / kThreads),
+                                kThreads, 0, s>>>(eng, ws.ctl, ws.u,
+                                                  ws.bins);
     } else if (!sys) {
         k_sorted_tile_sums<<<nt, kThreads, 0, s>>>(eng, ws.ctl,
-                                                   ws.u_tile_sum);
+                                                   ws.u_tile_sum, ws.u);
         k_sorted_spine<<<1, kSpineThreads, 0, s>>>(ws.u_tile_sum,
                                                    ws.u_tile_excl, ws.ctl);
         k_sorted_uniforms<<<nt, kThreads, 0, s>>>(eng, ws.ctl,
-                                                  ws.u_tile_excl, ws.u);
+                                                  ws.u_tile_excl, ws.u,
+                                                  ws.bins);
     }
-    cudaMemsetAsync(ws.lb_status, 0, sizeof(unsigned long long) * nt, s);
     const long long *kex = residual ? ws.tile_kexcl : nullptr;
 #define VSMC_INVERT(R, S)                                                     \
-    k_invert<W, R, S><<<nt, kThreads, 0, s>>>(wsrc, N, ws.ctl, ws.tile_excl,  \
-                                              kex, u, n_u, ws.lb_status,     \
-                                              rep_out, copy_from, ws.sinc)
+    k_invert<W, R, S><<<nt, kThreads, 0, s>>>(                                \
+        wsrc, N, ws.ctl, ws.tile_excl, kex, u, n_u, ws.bins, rep_out,        \
+        copy_from, ws.sinc, ws.tile_zeros, ws.tile_sinc_last)
     if (residual && sys)
         VSMC_INVERT(true, true);
     else if (residual)
@@ -985,8 +1172,11 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
     else
         VSMC_INVERT(false, false);
 #undef VSMC_INVERT
-    k_cfrp_fill<<<(unsigned)((N + kThreads - 1) / kThreads), kThreads, 0,
-                  s>>>(N, ws.ctl, ws.sinc, copy_from);
+    k_zero_spine<<<1, kSpineThreads, 0, s>>>(ws.tile_zeros, ws.tile_sinc_last,
+                                             ws.zexcl, ws.tfirst, ws.tlast,
+                                             nt, ws.ctl);
+    k_cfrp_fill<<<nt, kThreads, 0, s>>>(N, ws.ctl, ws.sinc, ws.zexcl,
+                                        ws.tfirst, ws.tlast, copy_from);
     k_resample_done<<<1, 1, 0, s>>>(ws.ctl);
 }
 

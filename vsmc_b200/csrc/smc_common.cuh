@@ -36,11 +36,11 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0,
             k0 += 0x9E3779B9u;
             k1 += 0xBB67AE85u;
         }
-        const uint32_t hi0 = __umulhi(0xCD9E8D57u, c.z);
-        const uint32_t lo1 = 0xCD9E8D57u * c.z;
-        const uint32_t hi2 = __umulhi(0xD2511F53u, c.x);
-        const uint32_t lo3 = 0xD2511F53u * c.x;
-        c = make_uint4(hi0 ^ k0 ^ c.y, lo1, hi2 ^ k1 ^ c.w, lo3);
+        // one 32x32->64 wide multiply gives both halves of each product
+        const unsigned long long pa = (unsigned long long)0xCD9E8D57u * c.z;
+        const unsigned long long pb = (unsigned long long)0xD2511F53u * c.x;
+        c = make_uint4((uint32_t)(pa >> 32) ^ k0 ^ c.y, (uint32_t)pa,
+                       (uint32_t)(pb >> 32) ^ k1 ^ c.w, (uint32_t)pb);
     }
     return c;
 }
@@ -136,11 +136,12 @@ __device__ __forceinline__ double canonical_u64(uint64_t x)
 
 // ... over a 32-bit engine: two words, (a + b * 2^32) * 2^-64 with a single
 // rounding of the sum.
+// The exact sum a + b*2^32 is the 64-bit integer (b << 32) | a, so its one
+// rounding to double is a single 64-bit conversion.
 __device__ __forceinline__ double canonical_u32x2(uint32_t a, uint32_t b)
 {
-    const double s = __dadd_rn(__uint2double_rn(a),
-                               __dmul_rn(__uint2double_rn(b), 4294967296.0));
-    const double r = __dmul_rn(s, 0x1p-64);
+    const unsigned long long x = ((unsigned long long)b << 32) | a;
+    const double r = __dmul_rn(__ull2double_rn(x), 0x1p-64);
     return r >= 1.0 ? 0x1.fffffffffffffp-1 : r;
 }
 
@@ -164,42 +165,32 @@ struct PhiloxStream {
     }
 };
 
-// One accepted polar pair (x*mult, y*mult) drawn exactly as libstdc++
-// normal_distribution::operator() does: x, y = 2U - 1; reject r2 > 1 or
-// r2 == 0; mult = sqrt(-2 log r2 / r2).  The first variate returned by the
-// distribution is y*mult, the cached second one x*mult.
-__device__ __forceinline__ void polar_pair_f64(PhiloxStream &s, double &first,
-                                               double &second)
+// One accepted point of libstdc++'s polar method (normal_distribution::
+// operator()): x, y = 2U - 1 from two canonical draws; reject r2 > 1 or
+// r2 == 0.  The acceptance test is exact double arithmetic on the same words
+// in both precision forms, so every form consumes the stream identically.
+__device__ __forceinline__ void polar_accept(PhiloxStream &s, double &x,
+                                             double &y, double &r2)
 {
-    double x, y, r2;
     do {
         const uint4 w = s.next_block();
         x = __dadd_rn(__dmul_rn(2.0, canonical_u32x2(w.x, w.y)), -1.0);
         y = __dadd_rn(__dmul_rn(2.0, canonical_u32x2(w.z, w.w)), -1.0);
         r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
     } while (r2 > 1.0 || r2 == 0.0);
-    const double mult = __dsqrt_rn(__ddiv_rn(__dmul_rn(-2.0, log(r2)), r2));
-    first = __dmul_rn(y, mult);
-    second = __dmul_rn(x, mult);
 }
 
-// Mixed form: the acceptance test runs in double on the same words, so the
-// stream position (and thus every later draw) is identical to the FP64 form;
-// only the transform runs in float.
-__device__ __forceinline__ void polar_pair_f32(PhiloxStream &s, float &first,
-                                               float &second)
+// mult = sqrt(-2 log(r2) / r2); the distribution returns y*mult first and
+// caches x*mult.
+__device__ __forceinline__ double polar_mult_f64(double r2)
 {
-    double x, y, r2;
-    do {
-        const uint4 w = s.next_block();
-        x = __dadd_rn(__dmul_rn(2.0, canonical_u32x2(w.x, w.y)), -1.0);
-        y = __dadd_rn(__dmul_rn(2.0, canonical_u32x2(w.z, w.w)), -1.0);
-        r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
-    } while (r2 > 1.0 || r2 == 0.0);
+    return __dsqrt_rn(__ddiv_rn(__dmul_rn(-2.0, log(r2)), r2));
+}
+
+__device__ __forceinline__ float polar_mult_f32(double r2)
+{
     const float r2f = static_cast<float>(r2);
-    const float mult = sqrtf(-2.0f * logf(r2f) / r2f);
-    first = static_cast<float>(y) * mult;
-    second = static_cast<float>(x) * mult;
+    return sqrtf(-2.0f * logf(r2f) / r2f);
 }
 
 // --------------------------------------------------------- reductions ------
