@@ -113,6 +113,28 @@ int vsmc_cuda_resample(int scheme, uint64_t N, const double *weight,
                        int32_t *copy_from, void *workspace,
                        size_t workspace_bytes, void *stream);
 
+/* Largest N accepted by vsmc_cuda_resample_noalloc. */
+#define VSMC_CUDA_NOALLOC_MAX_N 262144
+
+/* No counterpart in the reference.  vsmc_cuda_resample for callers that
+ * cannot allocate device memory (a fixed HBM budget reserved up front, loops
+ * where cudaMalloc/cudaFree would synchronise the device, or a plugin whose
+ * host owns every allocation): the same kernels and results, with the
+ * workspace (and the copy_from scratch when copy_from is NULL) taken from a
+ * static device array the library holds for N <= VSMC_CUDA_NOALLOC_MAX_N
+ * particles (about 4.1 MiB on every device that loads the library, kept
+ * until exit).  Larger N returns VSMC_CUDA_EINVAL.  It calls no cudaMalloc
+ * or cudaFree.  The first call on each device looks up the array's device
+ * address (cudaGetSymbolAddress, with that device current) and caches it;
+ * make that first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised by the
+ * caller. */
+int vsmc_cuda_resample_noalloc(int scheme, uint64_t N, const double *weight,
+                               const double *uniforms, uint64_t n_uniforms,
+                               vsmc_cuda_threefry_state *rng,
+                               int32_t *replication, int32_t *copy_from,
+                               void *stream);
+
 /* StateMatrix<ColMajor, dim, double>::copy(N, copy_from)
  * (include/vsmc/core/state_matrix.hpp:378-394): dst[d*N + i] =
  * src[d*N + copy_from[i]] for every column d (src != dst). */

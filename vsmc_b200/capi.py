@@ -68,6 +68,8 @@ def lib():
     L.vsmc_cuda_resample.argtypes = [i32, u64, vp, vp, u64, C.POINTER(ThreefryState),
                                      vp, vp, vp, C.c_size_t, vp]
     L.vsmc_cuda_copy_f64.argtypes = [u64, C.c_uint32, vp, vp, vp, vp]
+    L.vsmc_cuda_resample_noalloc.argtypes = [i32, u64, vp, vp, u64,
+                                             C.POINTER(ThreefryState), vp, vp, vp]
     L.vsmc_cuda_cv_config_default.argtypes = [C.POINTER(CVConfig)]
     L.vsmc_cuda_cv_config_default.restype = None
     L.vsmc_cuda_cv_device_bytes.argtypes = [C.POINTER(CVConfig)]
@@ -152,6 +154,20 @@ def resample(scheme, N, weight_ptr, rng: ThreefryState, rep_ptr, cf_ptr, ws_ptr,
     check(lib().vsmc_cuda_resample(scheme, N, weight_ptr, uniforms_ptr, n_uniforms,
                                    C.byref(rng), rep_ptr, cf_ptr, ws_ptr, ws_bytes, stream),
           "vsmc_cuda_resample")
+    return int(rng.offset - before)
+
+
+NOALLOC_MAX_N = 262144
+
+
+def resample_noalloc(scheme, N, weight_ptr, rng: ThreefryState, rep_ptr, cf_ptr,
+                     uniforms_ptr=None, n_uniforms=0, stream=None) -> int:
+    """vsmc_cuda_resample on the library's static scratch (no allocation);
+    N <= NOALLOC_MAX_N.  Returns the engine words drawn."""
+    before = rng.offset
+    check(lib().vsmc_cuda_resample_noalloc(scheme, N, weight_ptr, uniforms_ptr, n_uniforms,
+                                           C.byref(rng), rep_ptr, cf_ptr, stream),
+          "vsmc_cuda_resample_noalloc")
     return int(rng.offset - before)
 
 
