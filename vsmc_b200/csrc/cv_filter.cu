@@ -105,10 +105,8 @@ __device__ __forceinline__ void cv_particle(const CVParam &p, uint32_t iter,
                                             double &x, double &y, double &vx,
                                             double &vy, double, double)
 {
-    PhiloxStream s = particle_stream(iter, id, stream, k0, k1);
     double x1, y1, q1, x2, y2, q2;
-    polar_accept(s, x1, y1, q1);
-    polar_accept(s, x2, y2, q2);
+    polar_two(iter, id, stream, k0, k1, x1, y1, q1, x2, y2, q2);
     const double m1 = polar_mult_f64(q1);
     const double m2 = polar_mult_f64(q2);
     const double a = __dmul_rn(y1, m1), b = __dmul_rn(x1, m1);
@@ -153,10 +151,8 @@ __device__ __forceinline__ void cv_particle(const CVParam &p, uint32_t iter,
                                             float &y, float &vx, float &vy,
                                             double shx, double shy)
 {
-    PhiloxStream s = particle_stream(iter, id, stream, k0, k1);
     double x1, y1, q1, x2, y2, q2;
-    polar_accept(s, x1, y1, q1);
-    polar_accept(s, x2, y2, q2);
+    polar_two(iter, id, stream, k0, k1, x1, y1, q1, x2, y2, q2);
     if (Init) {
         // once per run: the prior in double, then stored as float offsets
         const double m1 = polar_mult_f64(q1), m2 = polar_mult_f64(q2);
@@ -187,33 +183,89 @@ __device__ __forceinline__ float cv_loglik(const CVParam &p, float x, float y,
 __device__ __forceinline__ double lse_exp(double v) { return exp(v); }
 __device__ __forceinline__ double lse_exp(float v) { return (double)expf(v); }
 
-// Accumulate one particle into the thread's online LSE state; `Real`
-// selects the exp precision.
+// Per-thread weight statistics against a lazy reference: the first finite
+// log-weight becomes the reference and later values are accumulated as
+// exp(lw - ref) even above it (double has the range), so the exponential is
+// evaluated once per particle; the reference moves only when a value
+// exceeds it by more than kLazy (then exp^2 could overflow).  mx tracks the
+// true maximum.
+struct LseRef {
+    double ref, mx, s1, s2, sx, sy;
+
+    __device__ __forceinline__ void init()
+    {
+        ref = -INFINITY;
+        mx = -INFINITY;
+        s1 = s2 = sx = sy = 0.0;
+    }
+};
+
 template <typename Real>
-__device__ __forceinline__ void lse_add(LseAcc &a, Real lw, Real x, Real y)
+struct LazyBound;
+template <>
+struct LazyBound<double> {
+    static constexpr double v = 300.0;
+};
+template <>
+struct LazyBound<float> {
+    static constexpr double v = 40.0;
+};
+
+template <typename Real>
+__device__ __forceinline__ void lse_add(LseRef &a, Real lw, Real x, Real y)
 {
     const double l = (double)lw;
-    if (!(l <= a.m)) {
-        if (l != l) {
-            a.s1 = l;
-            return;
-        }
-        a.rescale_to(l);
+    if (l != l) {
+        a.s1 = l; // NaN propagates to the degenerate check
+        return;
     }
     if (l == -INFINITY)
         return;
-    const double e = lse_exp((Real)(lw - (Real)a.m));
+    a.mx = fmax(a.mx, l);
+    if (a.ref == -INFINITY) {
+        a.ref = l;
+    } else if (l - a.ref > LazyBound<Real>::v) {
+        const double f = exp(a.ref - l);
+        a.s1 *= f;
+        a.s2 *= f * f;
+        a.sx *= f;
+        a.sy *= f;
+        a.ref = l;
+    }
+    const double e = lse_exp((Real)(lw - (Real)a.ref));
     a.s1 += e;
     a.s2 += e * e;
     a.sx += e * (double)x;
     a.sy += e * (double)y;
 }
 
-__device__ __forceinline__ void warp_merge(LseAcc &a, double &gx, double &gy,
-                                           unsigned width)
+// Rescale a thread's sums to the common maximum M: exp(ref - M) <= 1.
+__device__ __forceinline__ void lse_rescale(LseRef &a, double M)
+{
+    const double f = a.ref == -INFINITY ? 0.0 : exp(a.ref - M);
+    a.s1 *= f;
+    a.s2 *= f * f;
+    a.sx *= f;
+    a.sy *= f;
+    a.ref = M;
+}
+
+__device__ __forceinline__ double warp_max_nan(double v, unsigned width)
+{
+    for (unsigned o = width / 2; o > 0; o >>= 1)
+        v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Sum of the rescaled statistics over `width` lanes.
+__device__ __forceinline__ void warp_sum_stats(LseRef &a, double &gx,
+                                               double &gy, unsigned width)
 {
     for (unsigned o = width / 2; o > 0; o >>= 1) {
-        a.merge(shfl_xor(a, (int)o));
+        a.s1 += __shfl_xor_sync(0xffffffffu, a.s1, o);
+        a.s2 += __shfl_xor_sync(0xffffffffu, a.s2, o);
+        a.sx += __shfl_xor_sync(0xffffffffu, a.sx, o);
+        a.sy += __shfl_xor_sync(0xffffffffu, a.sy, o);
         gx += __shfl_xor_sync(0xffffffffu, gx, o);
         gy += __shfl_xor_sync(0xffffffffu, gy, o);
     }
@@ -233,8 +285,7 @@ k_cv_move(MoveArgs<Real> a)
     typedef typename Vec<Real>::type VT;
     constexpr int NW = kThreads / 32;
     // double-buffered warp partials: one barrier per tile
-    __shared__ LseAcc sh_acc[2][NW];
-    __shared__ double sh_g[2][2][NW];
+    __shared__ double sh_w[2][7][NW];
 
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int gather = Init ? 0 : a.ctl->resampled;
@@ -251,7 +302,7 @@ k_cv_move(MoveArgs<Real> a)
 
     for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
         const long long base = (long long)tile * kTile;
-        LseAcc acc;
+        LseRef acc;
         acc.init();
         double gx = 0.0, gy = 0.0;
 #pragma unroll 1
@@ -341,27 +392,42 @@ k_cv_move(MoveArgs<Real> a)
                 }
             }
         }
-        warp_merge(acc, gx, gy, 32);
+        // warp: common maximum, one rescale per lane, plain sums
+        const double wm = warp_max_nan(acc.mx, 32);
+        lse_rescale(acc, wm);
+        warp_sum_stats(acc, gx, gy, 32);
         if (lane == 0) {
-            sh_acc[buf][wid] = acc;
-            sh_g[buf][0][wid] = gx;
-            sh_g[buf][1][wid] = gy;
+            double *w = &sh_w[buf][0][0];
+            w[0 * NW + wid] = wm;
+            w[1 * NW + wid] = acc.s1;
+            w[2 * NW + wid] = acc.s2;
+            w[3 * NW + wid] = acc.sx;
+            w[4 * NW + wid] = acc.sy;
+            w[5 * NW + wid] = gx;
+            w[6 * NW + wid] = gy;
         }
         __syncthreads();
         if (wid == 0) {
-            LseAcc r;
+            const double *w = &sh_w[buf][0][0];
+            LseRef r;
             double tx = 0.0, ty = 0.0;
+            r.init();
             if (lane < NW) {
-                r = sh_acc[buf][lane];
-                tx = sh_g[buf][0][lane];
-                ty = sh_g[buf][1][lane];
-            } else {
-                r.init();
+                r.ref = w[0 * NW + lane];
+                r.mx = r.ref;
+                r.s1 = w[1 * NW + lane];
+                r.s2 = w[2 * NW + lane];
+                r.sx = w[3 * NW + lane];
+                r.sy = w[4 * NW + lane];
+                tx = w[5 * NW + lane];
+                ty = w[6 * NW + lane];
             }
-            warp_merge(r, tx, ty, NW);
+            const double tm = warp_max_nan(r.mx, NW);
+            lse_rescale(r, tm);
+            warp_sum_stats(r, tx, ty, NW);
             if (lane == 0) {
                 TileStats ts;
-                ts.m = r.m;
+                ts.m = tm;
                 ts.s1 = r.s1;
                 ts.s2 = r.s2;
                 ts.sx = r.sx;
@@ -400,24 +466,29 @@ struct FinalizeArgs {
 };
 
 constexpr int kFinalThreads = 1024;
+constexpr int kFinalSmemTiles = 16384; // spine staged in shared memory
 
-// One CTA, deterministic (contiguous runs of tiles per thread, fixed
-// reduction trees): pass 1 the global maximum M, pass 2 the rescaled sums
-// s1_t exp(m_t - M) etc. (independent exponentials, no serial chain), then
-// the decisions of Sampler::do_resample and the weight spine.
+// One CTA, deterministic.  Pass 1 (striped, coalesced loads): the global
+// maximum M.  Pass 2 (striped): the rescaled sums s1_t exp(m_t - M) etc.
+// with independent exponentials, and each tile's share of the normalised
+// weight mass stored for the spine.  Then the decisions of
+// Sampler::do_resample and the ordered exclusive spine over the stored
+// shares (contiguous runs per thread, read from shared memory).
 __global__ void __launch_bounds__(kFinalThreads) k_cv_finalize(FinalizeArgs a)
 {
     constexpr int NW = kFinalThreads / 32;
-    __shared__ double sh[7][NW];
+    extern __shared__ double agg[]; // ntiles shares (when staged)
+    __shared__ double sh[6][NW];
     __shared__ double sh_spine[NW];
     __shared__ int sh_res;
     __shared__ double sh_M, sh_coeff;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int per = (a.ntiles + blockDim.x - 1) / blockDim.x;
-    const int b = threadIdx.x * per, e = min(b + per, a.ntiles);
+    const int nt = a.ntiles;
+    const bool staged = nt <= kFinalSmemTiles;
+    double *share = staged ? agg : a.tile_excl; // scratch when not staged
     // pass 1: maximum (NaN propagates)
     double m = -INFINITY;
-    for (int t = b; t < e; ++t) {
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
         const double mt = a.ts[t].m, st = a.ts[t].s1;
         m = (mt != mt || st != st) ? NAN : (m != m ? m : fmax(m, mt));
     }
@@ -436,12 +507,14 @@ __global__ void __launch_bounds__(kFinalThreads) k_cv_finalize(FinalizeArgs a)
     }
     __syncthreads();
     const double M = sh_M;
-    // pass 2: sums rescaled to M
-    double v[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int t = b; t < e; ++t) {
+    // pass 2: sums rescaled to M; shares exp(m_t - M) s1_t (unnormalised)
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
         const TileStats ts = a.ts[t];
         const double f = ts.m == -INFINITY ? 0.0 : exp(ts.m - M);
-        v[0] += ts.s1 * f;
+        const double s1 = ts.s1 * f;
+        share[t] = s1;
+        v[0] += s1;
         v[1] += ts.s2 * f * f;
         v[2] += ts.sx * f;
         v[3] += ts.sy * f;
@@ -505,20 +578,23 @@ __global__ void __launch_bounds__(kFinalThreads) k_cv_finalize(FinalizeArgs a)
     __syncthreads();
     if (!sh_res || a.residual)
         return;
-    // weight spine for the resampling scan: tile t holds
-    // exp(m_t - M) * s1_t / S1 of the normalised weight mass
+    // ordered exclusive spine of the normalised shares
     const double coeff = sh_coeff;
+    const int per = (nt + blockDim.x - 1) / blockDim.x;
+    const int b = threadIdx.x * per, e = min(b + per, nt);
     double run = 0.0;
     for (int t = b; t < e; ++t)
-        run += exp(a.ts[t].m - M) * a.ts[t].s1 * coeff;
+        run += share[t] * coeff;
     double total;
     double off = block_excl_scan(run, sh_spine, total);
+    // in place when the shares live in tile_excl: read before write per t
     for (int t = b; t < e; ++t) {
+        const double x = share[t] * coeff;
         a.tile_excl[t] = off;
-        off += exp(a.ts[t].m - M) * a.ts[t].s1 * coeff;
+        off += x;
     }
     if (threadIdx.x == blockDim.x - 1)
-        a.tile_excl[a.ntiles] = total;
+        a.tile_excl[nt] = total;
     if (threadIdx.x == 0) {
         ResampleCtl *rc = a.rctl;
         rc->NN = a.N;
@@ -741,7 +817,10 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
     fa.residual = residual;
     fa.sys = sys;
     fa.eng = f->eng;
-    k_cv_finalize<<<1, kFinalThreads, 0, s>>>(fa);
+    const size_t fin_smem = f->ntiles <= kFinalSmemTiles
+                                ? (size_t)f->ntiles * sizeof(double)
+                                : 0;
+    k_cv_finalize<<<1, kFinalThreads, fin_smem, s>>>(fa);
 
     WeightsFromLog<Real> w;
     w.lw = static_cast<const Real *>(f->lw);
@@ -927,6 +1006,9 @@ int vsmc_cuda_cv_create(const vsmc_cuda_cv_config *cfg, void *stream,
     if (per < 1)
         per = 1;
     const long long g = (long long)sms * per;
+    cudaFuncSetAttribute(k_cv_finalize,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kFinalSmemTiles * (int)sizeof(double));
     f->move_grid = (int)(f->ntiles < g ? f->ntiles : g);
     e = cudaMemsetAsync(f->mem, 0, f->bytes, f->stream);
     if (e != cudaSuccess) {

@@ -806,27 +806,40 @@ k_zero_spine(const int32_t *tile_zeros, const int32_t *tile_sinc_last,
     if (!ctl->active)
         return;
     __shared__ long long sh[kSpineThreads / 32];
-    __shared__ int32_t E[kSpineStage];
+    __shared__ int32_t S[kSpineStage]; // zero counts, then surplus ends E
+    const bool staged = ntiles <= kSpineStage;
+    // phase 1: exclusive prefix of the zero counts (striped load, ordered
+    // contiguous runs from shared memory)
+    if (staged) {
+        for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
+            S[t] = tile_zeros[t];
+        __syncthreads();
+    }
+    const int32_t *Z = staged ? S : tile_zeros;
     const int per = (ntiles + blockDim.x - 1) / blockDim.x;
     const int b = threadIdx.x * per;
     const int e = min(b + per, ntiles);
     long long run = 0;
     for (int t = b; t < e; ++t)
-        run += tile_zeros[t];
+        run += Z[t];
     long long total;
     run = block_excl_scan(run, sh, total);
     for (int t = b; t < e; ++t) {
+        const int32_t z = Z[t];
         zexcl[t] = (int32_t)run;
-        if (t < kSpineStage)
-            E[t] = (int32_t)(tile_sinc_last[t] + run);
-        run += tile_zeros[t];
+        run += z;
     }
     if (threadIdx.x == blockDim.x - 1)
         zexcl[ntiles] = (int32_t)total;
     __syncthreads();
-    const bool staged = ntiles <= kSpineStage;
+    // phase 2: E[t] = surplus count at the end of tile t (non-decreasing)
+    if (staged) {
+        for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
+            S[t] = tile_sinc_last[t] + zexcl[t];
+        __syncthreads();
+    }
     auto Eat = [&](int t) {
-        return staged ? (long long)E[t]
+        return staged ? (long long)S[t]
                       : (long long)tile_sinc_last[t] + zexcl[t];
     };
     auto first_tile_above = [&](long long k) {
@@ -840,9 +853,10 @@ k_zero_spine(const int32_t *tile_zeros, const int32_t *tile_sinc_last,
         }
         return lo;
     };
+    // phase 3: the parent tiles of each tile's zero slots
     for (int t = threadIdx.x; t < ntiles; t += blockDim.x) {
         const long long z0 = zexcl[t];
-        const long long z1 = t + 1 < ntiles ? (long long)zexcl[t + 1] : total;
+        const long long z1 = zexcl[t + 1];
         if (z0 == z1) {
             tfirst[t] = 0;
             tlast[t] = -1;

@@ -180,6 +180,79 @@ __device__ __forceinline__ void polar_accept(PhiloxStream &s, double &x,
     } while (r2 > 1.0 || r2 == 0.0);
 }
 
+// Exact polar point of one Philox block (two canonical doubles).
+__device__ __forceinline__ void polar_point(const uint4 &w, double &x,
+                                            double &y, double &r2)
+{
+    x = __dadd_rn(__dmul_rn(2.0, canonical_u32x2(w.x, w.y)), -1.0);
+    y = __dadd_rn(__dmul_rn(2.0, canonical_u32x2(w.z, w.w)), -1.0);
+    r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+}
+
+__device__ __forceinline__ bool polar_ok(double r2)
+{
+    return !(r2 > 1.0 || r2 == 0.0);
+}
+
+// The first two accepted polar points of a particle stream (libstdc++'s
+// two calls of the polar loop).  Three blocks are drawn up front: their
+// Philox chains are independent, so they overlap in the pipeline, and 88%
+// of particles need no more; the rest continue one block at a time.  The
+// points are exactly those of the sequential loop, in stream order.
+__device__ __forceinline__ void polar_two(uint32_t iter, uint32_t id,
+                                          uint32_t stream, uint32_t k0,
+                                          uint32_t k1, double &x1, double &y1,
+                                          double &q1, double &x2, double &y2,
+                                          double &q2)
+{
+    uint4 w[3];
+    double x[3], y[3], r[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        w[k] = philox4x32_10(make_uint4((uint32_t)(k + 1), iter, id, stream),
+                             k0, k1);
+        polar_point(w[k], x[k], y[k], r[k]);
+    }
+    int n = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (polar_ok(r[k])) {
+            if (n == 0) {
+                x1 = x[k];
+                y1 = y[k];
+                q1 = r[k];
+            } else if (n == 1) {
+                x2 = x[k];
+                y2 = y[k];
+                q2 = r[k];
+            }
+            ++n;
+        }
+    }
+    if (n < 2) {
+        PhiloxStream s;
+        s.ctr = make_uint4(3u, iter, id, stream);
+        s.k0 = k0;
+        s.k1 = k1;
+        double a, b, c;
+        while (n < 2) {
+            polar_point(s.next_block(), a, b, c);
+            if (polar_ok(c)) {
+                if (n == 0) {
+                    x1 = a;
+                    y1 = b;
+                    q1 = c;
+                } else {
+                    x2 = a;
+                    y2 = b;
+                    q2 = c;
+                }
+                ++n;
+            }
+        }
+    }
+}
+
 // mult = sqrt(-2 log(r2) / r2); the distribution returns y*mult first and
 // caches x*mult.
 __device__ __forceinline__ double polar_mult_f64(double r2)
