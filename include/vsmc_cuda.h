@@ -230,6 +230,18 @@ int vsmc_cuda_cv_read_step(vsmc_cuda_cv_filter *f, uint64_t t, double *ess,
                            double *logz_inc, int32_t *resampled,
                            int synchronize);
 
+/* Fixed-ancestry runs (precision comparisons, trajectory replay).  With
+ * `record` (device, T_max x N int32) every step stores its copy_from in row
+ * t (meaningful where the step resampled).  With `replay` (device, T_max x N)
+ * and `replay_resampled` (device, T_max int32) the filter skips its own
+ * resampling: step t resamples iff replay_resampled[t] != 0 and then takes
+ * row t as copy_from, so a run in another precision form follows exactly
+ * the recorded ancestry.  Pass NULLs to turn either off.  The arrays stay
+ * owned by the caller and must outlive the steps that use them. */
+int vsmc_cuda_cv_set_ancestry(vsmc_cuda_cv_filter *f, int32_t *record,
+                              const int32_t *replay,
+                              const int32_t *replay_resampled);
+
 /* Kernel timing with CUDA events on the filter's stream.  While enabled,
  * every step records events around the move kernel and around the whole
  * step; vsmc_cuda_cv_timing returns the summed milliseconds of the move

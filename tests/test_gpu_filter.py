@@ -5,8 +5,8 @@ FP64 form: resampling decisions, resample-engine words and copy_from are
 exact; log-evidence, ESS and the posterior-mean path agree to 1e-9 relative
 (the moves differ from glibc only through log() in the polar normals and
 exp() in the weights, a few ulps).  Mixed form (float move/weights, double
-scan and log-evidence): log-evidence within 1e-4 relative of the FP64 oracle
-on this 1000-particle run."""
+scan and log-evidence): log-evidence within 1e-6 relative of the FP64 run on
+the same ancestry."""
 import numpy as np
 import pytest
 
@@ -15,7 +15,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 RTOL_FP64 = 1e-9
-RTOL_MIXED = 1e-4
+RTOL_MIXED = 1e-6
 
 
 @pytest.fixture(scope="module")
@@ -78,14 +78,61 @@ def test_fp64_large_against_oracle(capi, N, sch):
 
 
 @pytest.mark.parametrize("sch", [0, 3])
-def test_mixed_form(golden, capi, sch):
-    ox, oy = golden["cv_obs_x"], golden["cv_obs_y"]
-    h = run_gpu(capi, 1000, 100, sch, ox, oy, form=capi.MIXED)
-    ref = float(golden[f"cv_s{sch}_logz"])
-    err = abs(h["logz"] - ref) / abs(ref)
-    print(f"mixed form scheme {sch}: logZ {h['logz']:.10f} vs FP64 oracle {ref:.10f}, "
-          f"rel err {err:.3e}")
+def test_mixed_form_short_horizon(golden, capi, sch):
+    """Over a few steps the mixed form follows the FP64 ancestry exactly
+    (the polar acceptance is exact, positions are anchored on the
+    observation) and its log-evidence agrees to RTOL_MIXED."""
+    ox, oy = golden["cv_obs_x"][:5], golden["cv_obs_y"][:5]
+    a = run_gpu(capi, 1000, 5, sch, ox, oy)
+    b = run_gpu(capi, 1000, 5, sch, ox, oy, form=capi.MIXED)
+    assert np.array_equal(a["resampled"], b["resampled"])
+    err = abs(a["logz"] - b["logz"]) / abs(a["logz"])
+    print(f"mixed form, 5 steps, scheme {sch}: rel err {err:.3e}")
     assert err <= RTOL_MIXED
+
+
+def replay_pair(capi, N, T, sch, ox, oy):
+    """FP64 run recording its ancestry, then the mixed form replaying it."""
+    import torch
+
+    rec = torch.zeros((T, N), dtype=torch.int32, device="cuda")
+    with capi.CVFilter(N, T, scheme=sch) as f:
+        f.set_ancestry(record_ptr=rec.data_ptr())
+        f.set_observations_host(ox, oy)
+        f.initialize()
+        f.iterate(T - 1)
+        h64 = f.history()
+        z64 = f.log_evidence()
+    flags = torch.from_numpy(h64["resampled"].astype(np.int32)).cuda()
+    with capi.CVFilter(N, T, scheme=sch, form=capi.MIXED) as g:
+        g.set_ancestry(replay_ptr=rec.data_ptr(), replay_flags_ptr=flags.data_ptr())
+        g.set_observations_host(ox, oy)
+        g.initialize()
+        g.iterate(T - 1)
+        h32 = g.history()
+        z32 = g.log_evidence()
+    return z64, z32, h64, h32
+
+
+@pytest.mark.parametrize("N", [1000, 1 << 16])
+@pytest.mark.parametrize("sch", [0, 3])
+def test_mixed_form_fixed_ancestry(golden, capi, N, sch):
+    """Free-running, one ancestor flip from float rounding re-deals the
+    counter streams of every later slot (cfrp_trans order), so the two forms
+    soon sample different particles; their log-evidence then differs by
+    Monte Carlo noise.  The precision of the mixed form is its error on the
+    FP64 run's own ancestry: log-evidence within RTOL_MIXED (1e-6) over all
+    100 steps at N = 2^16 (3e-6 at N = 1000)."""
+    ox, oy = golden["cv_obs_x"], golden["cv_obs_y"]
+    z64, z32, h64, h32 = replay_pair(capi, N, 100, sch, ox, oy)
+    err = abs(z64 - z32) / abs(z64)
+    print(f"mixed form replay N={N} scheme {sch}: logZ {z32:.12f} vs FP64 {z64:.12f}, "
+          f"rel err {err:.3e}")
+    # At N = 1000 the weights concentrate on a handful of particles, so the
+    # float likelihood's rounding (about 1e-6 absolute per particle) is not
+    # averaged down: the bound there is 3e-6.
+    assert err <= (RTOL_MIXED if N >= 1 << 16 else 3e-6)
+    assert np.allclose(h32["mean_x"], h64["mean_x"], rtol=1e-5, atol=1e-5)
 
 
 def test_repeatable(golden, capi):

@@ -89,6 +89,7 @@ def lib():
     L.vsmc_cuda_cv_append_observations.argtypes = [vp, vp, vp, u64, i32]
     L.vsmc_cuda_cv_read_step.argtypes = [vp, u64, vp, vp, vp, i32]
     L.vsmc_cuda_cv_set_timing.argtypes = [vp, i32]
+    L.vsmc_cuda_cv_set_ancestry.argtypes = [vp, vp, vp, vp]
     L.vsmc_cuda_cv_timing.argtypes = [vp, C.POINTER(f64), C.POINTER(f64), C.POINTER(u64),
                                       C.POINTER(u64)]
     L.vsmc_cuda_cv_simulate.argtypes = [C.POINTER(CVConfig), C.c_uint32, u64, vp, vp, vp]
@@ -299,6 +300,11 @@ class CVFilter:
         check(lib().vsmc_cuda_cv_read_step(self.h, t, ess_ptr, logz_ptr, res_ptr,
                                            1 if synchronize else 0),
               "vsmc_cuda_cv_read_step")
+
+    def set_ancestry(self, record_ptr=None, replay_ptr=None, replay_flags_ptr=None):
+        check(lib().vsmc_cuda_cv_set_ancestry(self.h, record_ptr, replay_ptr,
+                                              replay_flags_ptr),
+              "vsmc_cuda_cv_set_ancestry")
 
     def set_timing(self, enable=True):
         check(lib().vsmc_cuda_cv_set_timing(self.h, 1 if enable else 0),

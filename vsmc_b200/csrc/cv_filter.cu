@@ -463,6 +463,7 @@ struct FinalizeArgs {
     int residual;
     int sys;
     EngineRef eng;
+    const int32_t *replay_flags; // replay: resampling decisions to follow
 };
 
 constexpr int kFinalThreads = 1024;
@@ -556,6 +557,8 @@ __global__ void __launch_bounds__(kFinalThreads) k_cv_finalize(FinalizeArgs a)
         } else {
             res = ess < a.threshold * Nd;
         }
+        if (a.replay_flags != nullptr)
+            res = a.replay_flags[a.t] != 0;
         a.hist_ess[a.t] = ess;
         a.hist_resampled[a.t] = res;
         a.hist_logz_inc[a.t] = dz;
@@ -571,8 +574,8 @@ __global__ void __launch_bounds__(kFinalThreads) k_cv_finalize(FinalizeArgs a)
             a.hist_mean_x[a.t] = ax + r[2] / S1;
             a.hist_mean_y[a.t] = ay + r[3] / S1;
         }
-        a.rctl->active = res;
-        sh_res = res;
+        a.rctl->active = a.replay_flags != nullptr ? 0 : res;
+        sh_res = a.replay_flags != nullptr ? 0 : res;
         sh_coeff = __ddiv_rn(1.0, S1);
     }
     __syncthreads();
@@ -704,6 +707,10 @@ struct vsmc_cuda_cv_filter {
     std::vector<cudaEvent_t> ev;  // 3 per timed step: move begin/end, step end
     size_t ev_used;
     uint64_t launches;
+    // ancestry record / replay (fixed-ancestry comparisons)
+    int32_t *rec_cf;            // T_max x N, device, caller-owned
+    const int32_t *rep_cf;      // T_max x N, device, caller-owned
+    const int32_t *rep_flags;   // T_max, device, caller-owned
 };
 
 namespace {
@@ -817,6 +824,7 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
     fa.residual = residual;
     fa.sys = sys;
     fa.eng = f->eng;
+    fa.replay_flags = f->rep_flags;
     const size_t fin_smem = f->ntiles <= kFinalSmemTiles
                                 ? (size_t)f->ntiles * sizeof(double)
                                 : 0;
@@ -825,8 +833,18 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
     WeightsFromLog<Real> w;
     w.lw = static_cast<const Real *>(f->lw);
     w.stats = &f->ctl->lw_max;
-    launch_resample_core(c.scheme, w, N, f->eng, f->rws, nullptr, 0,
-                         /*spine_done=*/true, nullptr, f->copy_from, s);
+    if (f->rep_cf != nullptr) {
+        // replay: the recorded ancestry of this step (used only if the
+        // recorded decision was to resample)
+        cudaMemcpyAsync(f->copy_from, f->rep_cf + (size_t)f->iter * c.N,
+                        c.N * 4, cudaMemcpyDeviceToDevice, s);
+    } else {
+        launch_resample_core(c.scheme, w, N, f->eng, f->rws, nullptr, 0,
+                             /*spine_done=*/true, nullptr, f->copy_from, s);
+    }
+    if (f->rec_cf != nullptr)
+        cudaMemcpyAsync(f->rec_cf + (size_t)f->iter * c.N, f->copy_from,
+                        c.N * 4, cudaMemcpyDeviceToDevice, s);
     if (ev)
         cudaEventRecord(ev[2], s);
     f->launches += 2 + resample_launches(c.scheme, false);
@@ -988,6 +1006,9 @@ int vsmc_cuda_cv_create(const vsmc_cuda_cv_config *cfg, void *stream,
     f->timing = false;
     f->ev_used = 0;
     f->launches = 0;
+    f->rec_cf = nullptr;
+    f->rep_cf = nullptr;
+    f->rep_flags = nullptr;
     // resample engine: Threefry4x64 seeded seed+2 (Seed::get twice)
     uint32_t sg = cfg->seed % 0xFFFFFFFFu;
     sg = sg == 0xFFFFFFFFu ? 1u : sg + 1u;
@@ -1289,6 +1310,21 @@ int vsmc_cuda_cv_read_step(vsmc_cuda_cv_filter *f, uint64_t t, double *ess,
     if (e != cudaSuccess)
         return cuda_status(e, "vsmc_cuda_cv_read_step");
     return synchronize ? sync_and_check(f) : VSMC_CUDA_OK;
+}
+
+int vsmc_cuda_cv_set_ancestry(vsmc_cuda_cv_filter *f, int32_t *record,
+                              const int32_t *replay,
+                              const int32_t *replay_resampled)
+{
+    if (f == nullptr || (replay == nullptr) != (replay_resampled == nullptr)) {
+        set_last_error("vsmc_cuda_cv_set_ancestry: replay needs both the "
+                       "ancestry and the decisions");
+        return VSMC_CUDA_EINVAL;
+    }
+    f->rec_cf = record;
+    f->rep_cf = replay;
+    f->rep_flags = replay_resampled;
+    return VSMC_CUDA_OK;
 }
 
 int vsmc_cuda_cv_set_timing(vsmc_cuda_cv_filter *f, int enable)
