@@ -268,6 +268,95 @@ int vsmc_cuda_cv_resample_words(vsmc_cuda_cv_filter *f, uint64_t *words);
 int vsmc_cuda_cv_copy_from(vsmc_cuda_cv_filter *f, int32_t *copy_from,
                            int32_t *resampled);
 
+/* ---- many filters on one device (batched runs and serving) -------------
+ *
+ * No counterpart in the reference, which runs one Sampler per filter
+ * (core/sampler.hpp:450-483) and leaves many-filter programs to loop over
+ * them.  A batch holds up to `capacity` constant-velocity filters in slots.
+ * Each slot keeps its particles, weights, RNG counters, resampling state,
+ * observations and histories resident in device memory (one allocation
+ * from the batch's own memory pool, admitted against `hbm_budget` bytes;
+ * 0 = no limit).  The scheme, form, threshold and model parameters come
+ * from `model` and are shared by every slot; N, T_max, seed and stream_id
+ * are per slot.  A step over a list of slots runs every listed filter's
+ * next step in one launch per kernel; each filter's results equal those of
+ * a vsmc_cuda_cv_filter with the same configuration, whatever else runs in
+ * the same launch.  All calls are asynchronous on `stream` unless noted,
+ * and the slot lists they take are copied before they return. */
+typedef struct vsmc_cuda_cv_batch vsmc_cuda_cv_batch;
+
+/* Device bytes one slot of N particles and T_max observations holds. */
+uint64_t vsmc_cuda_cv_batch_slot_bytes(const vsmc_cuda_cv_config *model,
+                                       uint64_t N, uint64_t T_max);
+
+int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
+                              uint32_t capacity, uint64_t hbm_budget,
+                              void *stream, vsmc_cuda_cv_batch **out);
+int vsmc_cuda_cv_batch_destroy(vsmc_cuda_cv_batch *b);
+
+/* Admits a filter (Sampler<T>(N, ...) plus Seed::set(seed)) into a free
+ * slot; VSMC_CUDA_ENOMEM when no slot is free or its bytes exceed the
+ * remaining budget.  The filter starts at step 0. */
+int vsmc_cuda_cv_batch_admit(vsmc_cuda_cv_batch *b, uint64_t N,
+                             uint64_t T_max, uint32_t seed,
+                             uint32_t stream_id, uint32_t *slot);
+
+/* Frees a slot and returns its bytes to the budget (the memory stays in
+ * the batch's pool for later admissions). */
+int vsmc_cuda_cv_batch_release(vsmc_cuda_cv_batch *b, uint32_t slot);
+int vsmc_cuda_cv_batch_bytes_in_use(vsmc_cuda_cv_batch *b, uint64_t *bytes);
+
+/* Observations of n slots, packed: slot k's T[k] values follow those of
+ * slots 0..k-1 in obs_x / obs_y (host or device memory).  Each series
+ * replaces the slot's observations from index 0. */
+int vsmc_cuda_cv_batch_set_observations(vsmc_cuda_cv_batch *b, uint32_t n,
+                                        const uint32_t *slots,
+                                        const uint64_t *T, const double *obs_x,
+                                        const double *obs_y, int on_device);
+
+/* One observation appended to each of n slots (host values). */
+int vsmc_cuda_cv_batch_append_observations(vsmc_cuda_cv_batch *b,
+                                           uint32_t n, const uint32_t *slots,
+                                           const double *x, const double *y);
+
+/* Restarts the listed filters at step 0 (Sampler::initialize's reset; the
+ * resample engine position is kept, as in the reference). */
+int vsmc_cuda_cv_batch_initialize(vsmc_cuda_cv_batch *b, uint32_t n,
+                                  const uint32_t *slots);
+
+/* One step of each listed filter: the first step of a filter is
+ * Sampler::initialize, later ones Sampler::iterate(1).  Every listed slot
+ * needs an observation for that step. */
+int vsmc_cuda_cv_batch_step(vsmc_cuda_cv_batch *b, uint32_t n,
+                            const uint32_t *slots);
+
+/* Steps each listed filter until its observations are used up (the whole
+ * run of a batch of series of different lengths). */
+int vsmc_cuda_cv_batch_run(vsmc_cuda_cv_batch *b, uint32_t n,
+                           const uint32_t *slots);
+
+/* The last step of each listed slot: ESS, log-evidence increment,
+ * resampled flag and running log-evidence (host arrays of n; each may be
+ * NULL).  Synchronises; returns a device error of any listed slot. */
+int vsmc_cuda_cv_batch_read_last(vsmc_cuda_cv_batch *b, uint32_t n,
+                                 const uint32_t *slots, double *ess,
+                                 double *logz_inc, int32_t *resampled,
+                                 double *log_evidence);
+
+int vsmc_cuda_cv_batch_iter_size(vsmc_cuda_cv_batch *b, uint32_t slot,
+                                 uint64_t *iter_size);
+
+/* Histories of one slot, as vsmc_cuda_cv_history.  Synchronises. */
+int vsmc_cuda_cv_batch_history(vsmc_cuda_cv_batch *b, uint32_t slot,
+                               double *ess, int32_t *resampled,
+                               double *logz_inc, double *mean_x,
+                               double *mean_y);
+
+int vsmc_cuda_cv_batch_synchronize(vsmc_cuda_cv_batch *b);
+
+/* Kernel launches this batch has issued. */
+int vsmc_cuda_cv_batch_launches(vsmc_cuda_cv_batch *b, uint64_t *launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,188 @@
+"""Many filters in one batch (vsmc_cuda_cv_batch).
+
+A filter's results must not depend on what else shares its launches: every
+slot of a batch equals a single vsmc_cuda_cv_filter with the same
+configuration bit for bit (histories, log-evidence), whether the batch runs
+all series to the end at once or advances filters one observation at a time
+in arbitrary groups, and the FP64 form of a slot matches the oracle's golden
+run within the single filter's tolerance."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+RTOL_FP64 = 1e-9
+KEYS = ("ess", "resampled", "logz_inc", "mean_x", "mean_y")
+
+# (N, T, seed, stream_id): ragged sizes around the 2048-particle tile
+SPECS = [(1000, 100, 101, 0), (2048, 12, 7, 1), (2049, 25, 8, 2), (5000, 40, 9, 3),
+         (300, 7, 10, 4), (16387, 20, 11, 5), (65536, 9, 12, 6), (2, 5, 13, 7)]
+
+
+@pytest.fixture(scope="module")
+def capi():
+    from vsmc_b200 import capi as C
+
+    C.lib()
+    return C
+
+
+def series(capi, golden, k, T, sid):
+    if k == 0:
+        return golden["cv_obs_x"][:T].copy(), golden["cv_obs_y"][:T].copy()
+    return capi.cv_simulate(T, obs_seed=100 + k, stream_id=sid)
+
+
+def single(capi, N, T, scheme, form, seed, sid, ox, oy):
+    with capi.CVFilter(N, T, scheme=scheme, form=form, seed=seed, stream_id=sid) as f:
+        f.set_observations_host(ox, oy)
+        f.initialize()
+        if T > 1:
+            f.iterate(T - 1)
+        h = f.history()
+        h["logz"] = f.log_evidence()
+    return h
+
+
+def assert_same(h, s, what):
+    for k in KEYS:
+        assert np.array_equal(h[k], s[k]), (what, k)
+
+
+@pytest.mark.parametrize("form", [0, 1])
+@pytest.mark.parametrize("scheme", range(6))
+def test_batch_run_equals_single(golden, capi, scheme, form):
+    obs = [series(capi, golden, k, T, sid) for k, (N, T, seed, sid) in enumerate(SPECS)]
+    with capi.CVBatch(len(SPECS), scheme=scheme, form=form) as b:
+        slots = [b.admit(N, T, seed, sid) for (N, T, seed, sid) in SPECS]
+        b.set_observations(slots, obs)
+        b.run(slots)
+        last = b.read_last(slots)
+        hist = [b.history(s) for s in slots]
+    for k, (N, T, seed, sid) in enumerate(SPECS):
+        s = single(capi, N, T, scheme, form, seed, sid, *obs[k])
+        assert_same(hist[k], s, (scheme, form, N))
+        assert last["log_evidence"][k] == s["logz"]
+        assert last["ess"][k] == s["ess"][-1]
+        assert last["resampled"][k] == s["resampled"][-1]
+    if form == 0:
+        h = hist[0]
+        assert np.array_equal(h["resampled"], golden[f"cv_s{scheme}_resampled"])
+        ref = golden[f"cv_s{scheme}_logz"]
+        assert abs(last["log_evidence"][0] - ref) <= RTOL_FP64 * abs(ref)
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_batch_streamed_equals_run(golden, capi, form):
+    """Serving order: filters admitted at different times, one observation
+    appended per step, ticks over random subsets; the results equal a run of
+    the same filters in one batch."""
+    scheme = 3
+    obs = [series(capi, golden, k, T, sid) for k, (N, T, seed, sid) in enumerate(SPECS)]
+    with capi.CVBatch(len(SPECS), scheme=scheme, form=form) as b:
+        slots = [b.admit(N, T, seed, sid) for (N, T, seed, sid) in SPECS]
+        b.set_observations(slots, obs)
+        b.run(slots)
+        ref = [b.history(s) for s in slots]
+        ref_logz = b.read_last(slots)["log_evidence"]
+    rng = np.random.default_rng(42)
+    with capi.CVBatch(len(SPECS) + 2, scheme=scheme, form=form) as b:
+        # two filler filters take the first slots, then leave
+        fill = [b.admit(4096, 50, 1, 90), b.admit(3000, 50, 2, 91)]
+        fobs = [capi.cv_simulate(50, obs_seed=7, stream_id=90 + i) for i in range(2)]
+        b.set_observations(fill, fobs)
+        b.step(fill)
+        pos = {}
+        slot_of = {}
+        pending = list(range(len(SPECS)))
+        rng.shuffle(pending)
+        admitted = []
+        released = False
+        while pending or any(pos[k] < SPECS[k][1] for k in admitted):
+            # admit up to two new filters per tick
+            for _ in range(min(2, len(pending))):
+                k = pending.pop()
+                N, T, seed, sid = SPECS[k]
+                slot_of[k] = b.admit(N, T, seed, sid)
+                pos[k] = 0
+                admitted.append(k)
+            live = [k for k in admitted if pos[k] < SPECS[k][1]]
+            tick = [k for k in live if rng.random() < 0.7] or live[:1]
+            sl = [slot_of[k] for k in tick]
+            b.append_observations(sl, [obs[k][0][pos[k]] for k in tick],
+                                  [obs[k][1][pos[k]] for k in tick])
+            b.step(sl + ([] if released else fill[:1]))
+            for k in tick:
+                pos[k] += 1
+            if not released and len(admitted) >= 4:
+                for f in fill:
+                    b.release(f)
+                released = True
+        got = [b.history(slot_of[k]) for k in range(len(SPECS))]
+        logz = b.read_last([slot_of[k] for k in range(len(SPECS))])["log_evidence"]
+    for k in range(len(SPECS)):
+        assert_same(got[k], ref[k], k)
+        assert logz[k] == ref_logz[k]
+
+
+def test_batch_admission_budget(capi):
+    with capi.CVBatch(3) as b0:
+        one = b0.slot_bytes(4096, 10)
+    assert one > 4096 * 80
+    with capi.CVBatch(3, hbm_budget=2 * one + one // 2) as b:
+        s0 = b.admit(4096, 10)
+        s1 = b.admit(4096, 10)
+        assert b.bytes_in_use() == 2 * one
+        with pytest.raises(capi.VsmcCudaError) as e:
+            b.admit(4096, 10)
+        assert e.value.status == capi.ENOMEM
+        small = b.admit(1024, 10)  # fits in the remaining half
+        with pytest.raises(capi.VsmcCudaError) as e:
+            b.admit(2, 1)  # every slot in use
+        assert e.value.status == capi.ENOMEM
+        b.release(s1)
+        s3 = b.admit(4096, 10)
+        assert s3 == s1
+        assert b.bytes_in_use() == 2 * one + b.slot_bytes(1024, 10)
+        del s0, small
+
+
+def test_batch_bad_calls(capi):
+    with capi.CVBatch(4) as b:
+        s = b.admit(1024, 3)
+        with pytest.raises(capi.VsmcCudaError) as e:
+            b.step([s])  # no observation yet
+        assert e.value.status == capi.EINVAL
+        b.set_observations([s], [capi.cv_simulate(3, obs_seed=1)])
+        with pytest.raises(capi.VsmcCudaError):
+            b.step([s, s])  # listed twice
+        with pytest.raises(capi.VsmcCudaError):
+            b.step([3])  # not admitted
+        with pytest.raises(capi.VsmcCudaError):
+            b.set_observations([s], [capi.cv_simulate(4, obs_seed=1)])  # > T_max
+        b.run([s])
+        assert b.iter_size(s) == 3
+        with pytest.raises(capi.VsmcCudaError):
+            b.step([s])  # observations used up
+        with pytest.raises(capi.VsmcCudaError):
+            b.append_observations([s], [0.0], [0.0])  # series full
+        b.initialize([s])
+        assert b.iter_size(s) == 0
+        b.run([s])
+        h = b.history(s)
+        assert h["ess"].size == 3 and np.all(np.isfinite(h["ess"]))
+
+
+def test_batch_nan_observation_is_degenerate(capi):
+    with capi.CVBatch(2) as b:
+        good, bad = b.admit(2048, 4, 1, 0), b.admit(2048, 4, 2, 1)
+        ox, oy = capi.cv_simulate(4, obs_seed=3)
+        bx = ox.copy()
+        bx[2] = np.nan
+        b.set_observations([good, bad], [(ox, oy), (bx, oy)])
+        b.run([good, bad])
+        r = b.read_last([good])
+        assert np.isfinite(r["log_evidence"][0])
+        with pytest.raises(capi.VsmcCudaError) as e:
+            b.read_last([good, bad])
+        assert e.value.status == capi.EDEGENERATE

@@ -93,6 +93,24 @@ def lib():
     L.vsmc_cuda_cv_timing.argtypes = [vp, C.POINTER(f64), C.POINTER(f64), C.POINTER(u64),
                                       C.POINTER(u64)]
     L.vsmc_cuda_cv_simulate.argtypes = [C.POINTER(CVConfig), C.c_uint32, u64, vp, vp, vp]
+    u32 = C.c_uint32
+    L.vsmc_cuda_cv_batch_slot_bytes.restype = u64
+    L.vsmc_cuda_cv_batch_slot_bytes.argtypes = [C.POINTER(CVConfig), u64, u64]
+    L.vsmc_cuda_cv_batch_create.argtypes = [C.POINTER(CVConfig), u32, u64, vp, C.POINTER(vp)]
+    L.vsmc_cuda_cv_batch_destroy.argtypes = [vp]
+    L.vsmc_cuda_cv_batch_admit.argtypes = [vp, u64, u64, u32, u32, C.POINTER(u32)]
+    L.vsmc_cuda_cv_batch_release.argtypes = [vp, u32]
+    L.vsmc_cuda_cv_batch_bytes_in_use.argtypes = [vp, C.POINTER(u64)]
+    L.vsmc_cuda_cv_batch_set_observations.argtypes = [vp, u32, vp, vp, vp, vp, i32]
+    L.vsmc_cuda_cv_batch_append_observations.argtypes = [vp, u32, vp, vp, vp]
+    L.vsmc_cuda_cv_batch_initialize.argtypes = [vp, u32, vp]
+    L.vsmc_cuda_cv_batch_step.argtypes = [vp, u32, vp]
+    L.vsmc_cuda_cv_batch_run.argtypes = [vp, u32, vp]
+    L.vsmc_cuda_cv_batch_read_last.argtypes = [vp, u32, vp, vp, vp, vp, vp]
+    L.vsmc_cuda_cv_batch_iter_size.argtypes = [vp, u32, C.POINTER(u64)]
+    L.vsmc_cuda_cv_batch_history.argtypes = [vp, u32, vp, vp, vp, vp, vp]
+    L.vsmc_cuda_cv_batch_synchronize.argtypes = [vp]
+    L.vsmc_cuda_cv_batch_launches.argtypes = [vp, C.POINTER(u64)]
     _lib = L
     return L
 
@@ -330,3 +348,148 @@ class CVFilter:
         check(lib().vsmc_cuda_cv_copy_from(self.h, _np_ptr(cf), C.byref(r)),
               "vsmc_cuda_cv_copy_from")
         return cf, bool(r.value)
+
+
+class CVBatch:
+    """Many constant-velocity filters resident on one device (slots).  The
+    scheme, form, threshold and model parameters are shared; N, T_max, seed
+    and stream_id are per slot.  ``step(slots)`` advances each listed filter
+    by one step in one launch per kernel; ``run(slots)`` steps each until its
+    observations are used up."""
+
+    def __init__(self, capacity, scheme=Multinomial, form=FP64, threshold=0.5,
+                 hbm_budget=0, stream=None, **params):
+        self.model = cv_config(N=2, T_max=1, scheme=scheme, form=form,
+                               threshold=threshold, **params)
+        self.capacity = capacity
+        self.stream = stream
+        h = C.c_void_p()
+        check(lib().vsmc_cuda_cv_batch_create(C.byref(self.model), capacity, hbm_budget,
+                                              stream, C.byref(h)),
+              "vsmc_cuda_cv_batch_create")
+        self.h = h
+        self.N = {}
+
+    def slot_bytes(self, N, T_max) -> int:
+        return int(lib().vsmc_cuda_cv_batch_slot_bytes(C.byref(self.model), N, T_max))
+
+    def close(self):
+        if getattr(self, "h", None):
+            check(lib().vsmc_cuda_cv_batch_destroy(self.h), "vsmc_cuda_cv_batch_destroy")
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @staticmethod
+    def _slots(slots):
+        import numpy as np
+        a = np.ascontiguousarray(np.atleast_1d(np.asarray(slots, dtype=np.uint32)))
+        return a, a.size
+
+    def admit(self, N, T_max, seed=101, stream_id=0) -> int:
+        s = C.c_uint32()
+        check(lib().vsmc_cuda_cv_batch_admit(self.h, N, T_max, seed, stream_id, C.byref(s)),
+              "vsmc_cuda_cv_batch_admit")
+        self.N[int(s.value)] = N
+        return int(s.value)
+
+    def release(self, slot):
+        check(lib().vsmc_cuda_cv_batch_release(self.h, slot), "vsmc_cuda_cv_batch_release")
+        self.N.pop(slot, None)
+
+    def bytes_in_use(self) -> int:
+        v = C.c_uint64()
+        check(lib().vsmc_cuda_cv_batch_bytes_in_use(self.h, C.byref(v)),
+              "vsmc_cuda_cv_batch_bytes_in_use")
+        return int(v.value)
+
+    def set_observations(self, slots, series):
+        """series: one (obs_x, obs_y) pair of float64 arrays per slot."""
+        import numpy as np
+        a, n = self._slots(slots)
+        T = np.array([len(x) for x, _ in series], np.uint64)
+        ox = np.ascontiguousarray(np.concatenate([x for x, _ in series]), np.float64)
+        oy = np.ascontiguousarray(np.concatenate([y for _, y in series]), np.float64)
+        check(lib().vsmc_cuda_cv_batch_set_observations(self.h, n, a.ctypes.data, T.ctypes.data,
+                                                        ox.ctypes.data, oy.ctypes.data, 0),
+              "vsmc_cuda_cv_batch_set_observations")
+
+    def set_observations_packed(self, slots, T, ox_ptr, oy_ptr, on_device):
+        import numpy as np
+        a, n = self._slots(slots)
+        Ta = np.ascontiguousarray(T, np.uint64)
+        check(lib().vsmc_cuda_cv_batch_set_observations(self.h, n, a.ctypes.data, Ta.ctypes.data,
+                                                        ox_ptr, oy_ptr, 1 if on_device else 0),
+              "vsmc_cuda_cv_batch_set_observations")
+
+    def append_observations(self, slots, x, y):
+        import numpy as np
+        a, n = self._slots(slots)
+        xa = np.ascontiguousarray(np.atleast_1d(x), np.float64)
+        ya = np.ascontiguousarray(np.atleast_1d(y), np.float64)
+        check(lib().vsmc_cuda_cv_batch_append_observations(self.h, n, a.ctypes.data,
+                                                           xa.ctypes.data, ya.ctypes.data),
+              "vsmc_cuda_cv_batch_append_observations")
+
+    def initialize(self, slots):
+        a, n = self._slots(slots)
+        check(lib().vsmc_cuda_cv_batch_initialize(self.h, n, a.ctypes.data),
+              "vsmc_cuda_cv_batch_initialize")
+
+    def step(self, slots):
+        a, n = self._slots(slots)
+        check(lib().vsmc_cuda_cv_batch_step(self.h, n, a.ctypes.data), "vsmc_cuda_cv_batch_step")
+
+    def run(self, slots):
+        a, n = self._slots(slots)
+        check(lib().vsmc_cuda_cv_batch_run(self.h, n, a.ctypes.data), "vsmc_cuda_cv_batch_run")
+
+    def read_last(self, slots):
+        """dict of ess, logz_inc, resampled, log_evidence (one entry per slot)."""
+        import numpy as np
+        a, n = self._slots(slots)
+        r = dict(ess=np.zeros(n), logz_inc=np.zeros(n), resampled=np.zeros(n, np.int32),
+                 log_evidence=np.zeros(n))
+        check(lib().vsmc_cuda_cv_batch_read_last(self.h, n, a.ctypes.data,
+                                                 *[_np_ptr(r[k]) for k in
+                                                   ("ess", "logz_inc", "resampled",
+                                                    "log_evidence")]),
+              "vsmc_cuda_cv_batch_read_last")
+        return r
+
+    def iter_size(self, slot) -> int:
+        v = C.c_uint64()
+        check(lib().vsmc_cuda_cv_batch_iter_size(self.h, slot, C.byref(v)),
+              "vsmc_cuda_cv_batch_iter_size")
+        return int(v.value)
+
+    def history(self, slot):
+        import numpy as np
+        T = self.iter_size(slot)
+        r = dict(ess=np.zeros(T), resampled=np.zeros(T, np.int32), logz_inc=np.zeros(T),
+                 mean_x=np.zeros(T), mean_y=np.zeros(T))
+        check(lib().vsmc_cuda_cv_batch_history(self.h, slot,
+                                               *[_np_ptr(r[k]) for k in
+                                                 ("ess", "resampled", "logz_inc",
+                                                  "mean_x", "mean_y")]),
+              "vsmc_cuda_cv_batch_history")
+        return r
+
+    def synchronize(self):
+        check(lib().vsmc_cuda_cv_batch_synchronize(self.h), "vsmc_cuda_cv_batch_synchronize")
+
+    def launches(self) -> int:
+        v = C.c_uint64()
+        check(lib().vsmc_cuda_cv_batch_launches(self.h, C.byref(v)),
+              "vsmc_cuda_cv_batch_launches")
+        return int(v.value)

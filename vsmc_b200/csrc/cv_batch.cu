@@ -1,0 +1,1226 @@
+// cv_batch.cu -- many independent constant-velocity Student-t filters held
+// on the device at once and stepped together.
+//
+// vSMC runs one Sampler per filter (core/sampler.hpp:450-483); a program
+// with many filters loops over them.  Here every filter lives in a slot of
+// one vsmc_cuda_cv_batch: its particles, weights, RNG counters, resampling
+// workspace, observations and histories stay resident in device memory
+// (one allocation per slot from the batch's own memory pool, admitted
+// against a byte budget).  A step over a list of slots is one launch per
+// kernel of the single-filter step (cv_kernels.cuh, resample.cuh) with
+// the grid flattened over all (slot, tile) pairs: each CTA looks up its
+// slot and tile in a map, reads the slot's record and runs the same
+// per-tile body as the single-filter kernel.  Results therefore do not
+// depend on which other filters share a launch, and equal those of a
+// single filter with the same configuration bit for bit.
+//
+// Each slot keeps its own step count on the device, so one launch can mix
+// filters at different steps (serving: each filter advances when its next
+// observation arrives) and filters that start (step 0 runs the prior).
+#include "cv_kernels.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace vsmc_b200 {
+
+void set_last_error(const std::string &msg);
+int cuda_status(cudaError_t e, const char *what);
+
+// Device record of one filter slot.
+struct BatchSlot {
+    void *state[2][4]; // step t writes state[t & 1]
+    void *lw;
+    int32_t *copy_from;
+    FilterCtl *ctl;
+    TileStats *tile_stats;
+    double *obs_x, *obs_y;
+    double *hist_ess, *hist_logz_inc, *hist_mean_x, *hist_mean_y;
+    int32_t *hist_resampled;
+    ResampleWorkspace rws;
+    EngineRef eng;
+    long long N;
+    long long T_max;
+    long long t; // steps done; advanced by the last kernel of each step
+    int ntiles;
+    uint32_t k0, stream_id;
+};
+
+// Flattened grid: CTA b of a tile kernel works on tile `tile` of `slot`.
+struct TileRef {
+    int32_t slot;
+    int32_t tile;
+};
+
+// Settings shared by every filter of a batch.
+struct BatchConst {
+    CVParam p;
+    double threshold;
+    int residual, sys, anchored;
+};
+
+template <typename Real>
+__device__ __forceinline__ MoveArgs<Real> batch_move_args(const BatchSlot &b,
+                                                          const CVParam &p)
+{
+    MoveArgs<Real> a;
+    const int out = (int)(b.t & 1), in = (int)((b.t + 1) & 1);
+    for (int d = 0; d < 4; ++d) {
+        a.in[d] = static_cast<const Real *>(b.state[in][d]);
+        a.out[d] = static_cast<Real *>(b.state[out][d]);
+    }
+    a.lw = static_cast<Real *>(b.lw);
+    a.copy_from = b.copy_from;
+    a.ctl = b.ctl;
+    a.obs_x = b.obs_x;
+    a.obs_y = b.obs_y;
+    a.tile_stats = b.tile_stats;
+    a.N = b.N;
+    a.ntiles = b.ntiles;
+    a.iter = (uint32_t)b.t;
+    a.k0 = b.k0;
+    a.k1 = 0;
+    a.stream = b.stream_id;
+    a.p = p;
+    return a;
+}
+
+template <typename Real>
+__device__ __forceinline__ WeightsFromLog<Real> batch_weights(
+    const BatchSlot &b)
+{
+    WeightsFromLog<Real> w;
+    w.lw = static_cast<const Real *>(b.lw);
+    w.stats = &b.ctl->lw_max;
+    return w;
+}
+
+// CTA per work item: the map entries of its slot's tiles.
+static __global__ void kb_expand(const BatchSlot *slots, const int32_t *work,
+                                 const int32_t *tile0, int n, TileRef *map)
+{
+    const int w = blockIdx.x;
+    if (w >= n)
+        return;
+    const int slot = work[w];
+    const int nt = slots[slot].ntiles;
+    for (int k = threadIdx.x; k < nt; k += blockDim.x)
+        map[tile0[w] + k] = TileRef{slot, k};
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(kThreads, VSMC_MOVE_MIN_BLOCKS)
+kb_move(const BatchSlot *slots, const TileRef *map, CVParam p)
+{
+    __shared__ double sh_w[7 * kMoveWarps];
+    const TileRef r = map[blockIdx.x];
+    const BatchSlot &b = slots[r.slot];
+    const MoveArgs<Real> a = batch_move_args<Real>(b, p);
+    if (a.iter == 0) {
+        const MoveStep<Real> ms = move_step<Real, true>(a);
+        cv_move_tile<Real, true>(a, ms, r.tile, sh_w);
+    } else {
+        const MoveStep<Real> ms = move_step<Real, false>(a);
+        cv_move_tile<Real, false>(a, ms, r.tile, sh_w);
+    }
+}
+
+constexpr int kBatchAgg = 2048; // tile shares staged in shared memory
+
+static __global__ void __launch_bounds__(kFinalThreads)
+kb_finalize(const BatchSlot *slots, const int32_t *work, BatchConst c)
+{
+    __shared__ SmemFinal sm;
+    __shared__ double agg[kBatchAgg];
+    const BatchSlot &b = slots[work[blockIdx.x]];
+    FinalizeArgs a;
+    a.ctl = b.ctl;
+    a.ts = b.tile_stats;
+    a.ntiles = b.ntiles;
+    a.N = b.N;
+    a.threshold = c.threshold;
+    a.t = b.t;
+    a.init = b.t == 0;
+    a.anchored = c.anchored;
+    a.obs_x = b.obs_x;
+    a.obs_y = b.obs_y;
+    a.hist_ess = b.hist_ess;
+    a.hist_resampled = b.hist_resampled;
+    a.hist_logz_inc = b.hist_logz_inc;
+    a.hist_mean_x = b.hist_mean_x;
+    a.hist_mean_y = b.hist_mean_y;
+    a.rctl = b.rws.ctl;
+    a.tile_excl = b.rws.tile_excl;
+    a.residual = c.residual;
+    a.sys = c.sys;
+    a.eng = b.eng;
+    a.replay_flags = nullptr;
+    k_cv_finalize_body(a, agg, kBatchAgg, sm);
+}
+
+template <typename Real, bool Residual>
+__global__ void __launch_bounds__(kThreads)
+kb_tile_sums(const BatchSlot *slots, const TileRef *map)
+{
+    __shared__ SmemTileSums sm;
+    const TileRef r = map[blockIdx.x];
+    const BatchSlot &b = slots[r.slot];
+    k_tile_sums_body<WeightsFromLog<Real>, Residual>(
+        batch_weights<Real>(b), b.N, b.rws.ctl, b.rws.tile_sum,
+        Residual ? b.rws.tile_k : nullptr, r.tile, sm);
+}
+
+template <bool Residual, bool Sys>
+__global__ void __launch_bounds__(kSpineThreads)
+kb_spine_weights(const BatchSlot *slots, const int32_t *work)
+{
+    __shared__ SmemSpine sm;
+    const BatchSlot &b = slots[work[blockIdx.x]];
+    k_spine_weights_body<Residual, Sys>(
+        b.rws.tile_sum, Residual ? b.rws.tile_k : nullptr, b.rws.tile_excl,
+        Residual ? b.rws.tile_kexcl : nullptr, b.ntiles, b.N, b.eng,
+        b.rws.ctl, 0, sm);
+}
+
+// Stratified uniforms: the single-filter kernel runs one thread per block
+// of 4 uniforms over N / 4 + 2 blocks; here the CTA of tile k covers blocks
+// [512 k, 512 (k + 1)) and the last tile the remainder, every warp whole.
+static __global__ void __launch_bounds__(kThreads)
+kb_uniforms_stratified(const BatchSlot *slots, const TileRef *map)
+{
+    __shared__ SmemNone sm;
+    const TileRef r = map[blockIdx.x];
+    const BatchSlot &b = slots[r.slot];
+    constexpr long long per = kTile / 4;
+    const long long lo = (long long)r.tile * per;
+    const long long hi =
+        r.tile == b.ntiles - 1 ? b.N / 4 + 2 : lo + per;
+    for (long long g = lo; g < hi; g += kThreads)
+        k_uniforms_stratified_body(b.eng, b.rws.ctl, b.rws.u, b.rws.bins,
+                                   (unsigned long long)(g + threadIdx.x), sm);
+}
+
+static __global__ void __launch_bounds__(kThreads)
+kb_sorted_tile_sums(const BatchSlot *slots, const TileRef *map)
+{
+    __shared__ SmemSortedSums sm;
+    const TileRef r = map[blockIdx.x];
+    const BatchSlot &b = slots[r.slot];
+    k_sorted_tile_sums_body(b.eng, b.rws.ctl, b.rws.u_tile_sum, b.rws.u,
+                            r.tile, sm);
+}
+
+static __global__ void __launch_bounds__(kSpineThreads)
+kb_sorted_spine(const BatchSlot *slots, const int32_t *work)
+{
+    __shared__ SmemSpine sm;
+    const BatchSlot &b = slots[work[blockIdx.x]];
+    k_sorted_spine_body(b.rws.u_tile_sum, b.rws.u_tile_excl, b.rws.ctl, 0,
+                        sm);
+}
+
+static __global__ void __launch_bounds__(kThreads)
+kb_sorted_uniforms(const BatchSlot *slots, const TileRef *map)
+{
+    __shared__ SmemSortedUniforms sm;
+    const TileRef r = map[blockIdx.x];
+    const BatchSlot &b = slots[r.slot];
+    k_sorted_uniforms_body(b.eng, b.rws.ctl, b.rws.u_tile_excl, b.rws.u,
+                           b.rws.bins, r.tile, sm);
+}
+
+template <typename Real, bool Residual, bool Sys>
+__global__ void __launch_bounds__(kThreads)
+kb_invert(const BatchSlot *slots, const TileRef *map)
+{
+    __shared__ SmemInvert<Residual> sm;
+    const TileRef r = map[blockIdx.x];
+    const BatchSlot &b = slots[r.slot];
+    k_invert_body<WeightsFromLog<Real>, Residual, Sys>(
+        batch_weights<Real>(b), b.N, b.rws.ctl, b.rws.tile_excl,
+        Residual ? b.rws.tile_kexcl : nullptr, b.rws.u, b.N, b.rws.bins,
+        nullptr, b.copy_from, b.rws.sinc, b.rws.tile_zeros,
+        b.rws.tile_sinc_last, r.tile, sm);
+}
+
+static __global__ void __launch_bounds__(kSpineThreads)
+kb_zero_spine(const BatchSlot *slots, const int32_t *work)
+{
+    __shared__ SmemZeroSpine sm;
+    const BatchSlot &b = slots[work[blockIdx.x]];
+    k_zero_spine_body(b.rws.tile_zeros, b.rws.tile_sinc_last, b.rws.zexcl,
+                      b.rws.tfirst, b.rws.tlast, b.ntiles, b.rws.ctl, 0, sm);
+}
+
+static __global__ void __launch_bounds__(kThreads)
+kb_cfrp_fill(const BatchSlot *slots, const TileRef *map)
+{
+    __shared__ SmemFill sm;
+    const TileRef r = map[blockIdx.x];
+    const BatchSlot &b = slots[r.slot];
+    k_cfrp_fill_body(b.N, b.rws.ctl, b.rws.sinc, b.rws.zexcl, b.rws.tfirst,
+                     b.rws.tlast, b.copy_from, r.tile, sm);
+}
+
+// End of a step: the resample engine position (k_resample_done) and the
+// slot's step count.
+static __global__ void kb_step_done(BatchSlot *slots, const int32_t *work,
+                                    int n)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= n)
+        return;
+    BatchSlot &b = slots[work[w]];
+    ResampleCtl *c = b.rws.ctl;
+    if (c->active)
+        c->offset += c->words;
+    b.t += 1;
+}
+
+// Fresh filter state (Sampler::initialize's reset): step count 0, cleared
+// control block; the resample engine position is kept.
+__device__ __forceinline__ void reset_slot(BatchSlot &b)
+{
+    FilterCtl h;
+    h.lw_max = 0.0;
+    h.s1 = 0.0;
+    h.s2 = 0.0;
+    h.ess = 0.0;
+    h.logz = 0.0;
+    h.resampled = 0;
+    h.error = 0;
+    h.monitor_done = -1;
+    *b.ctl = h;
+    b.t = 0;
+}
+
+static __global__ void kb_reset(BatchSlot *slots, const int32_t *work, int n)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w < n)
+        reset_slot(slots[work[w]]);
+}
+
+static __global__ void kb_reset_slot(BatchSlot *slots, int slot)
+{
+    if (threadIdx.x == 0)
+        reset_slot(slots[slot]);
+}
+
+// Observations: record k writes obs[index] of `slot`.
+struct ObsRecord {
+    int32_t slot;
+    int32_t count;  // values to copy from `src` (set) or 1 (append)
+    long long index; // first index written
+    long long src;   // offset in the packed source arrays
+};
+
+static __global__ void kb_scatter_obs(const BatchSlot *slots,
+                                      const ObsRecord *rec, const double *sx,
+                                      const double *sy)
+{
+    const ObsRecord r = rec[blockIdx.x];
+    const BatchSlot &b = slots[r.slot];
+    for (int k = threadIdx.x; k < r.count; k += blockDim.x) {
+        b.obs_x[r.index + k] = sx[r.src + k];
+        b.obs_y[r.index + k] = sy[r.src + k];
+    }
+}
+
+// Summary of each work item's last step: ess, log-evidence increment,
+// resampled flag, running log-evidence, error code.
+static __global__ void kb_read_last(const BatchSlot *slots,
+                                    const int32_t *work, int n, double *out)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= n)
+        return;
+    const BatchSlot &b = slots[work[w]];
+    const long long t = b.t - 1;
+    double *o = out + 5 * (long long)w;
+    if (t < 0) {
+        o[0] = o[1] = o[2] = o[3] = 0.0;
+    } else {
+        o[0] = b.hist_ess[t];
+        o[1] = b.hist_logz_inc[t];
+        o[2] = (double)b.hist_resampled[t];
+        o[3] = b.ctl->logz;
+    }
+    const int e = b.ctl->error != 0 ? b.ctl->error : b.rws.ctl->error;
+    o[4] = (double)e;
+}
+
+// Monitor of a slot's last step when it resampled and no later move has
+// gathered it.  Same association as k_cv_monitor_gather over kMonParts
+// CTAs of kThreads followed by k_cv_monitor_finish.
+constexpr int kMonParts = 1184;
+
+template <typename Real>
+__global__ void __launch_bounds__(kThreads)
+kb_monitor_flush(const BatchSlot *slots, const int32_t *work, int anchored)
+{
+    __shared__ double sh[2][kThreads / 32];
+    const BatchSlot &b = slots[work[blockIdx.x]];
+    const long long t = b.t - 1;
+    if (t < 0 || !b.ctl->resampled || b.ctl->monitor_done == t)
+        return;
+    const long long N = b.N;
+    const long long stride = (long long)kMonParts * kThreads;
+    const Real *x = static_cast<const Real *>(b.state[t & 1][0]);
+    const Real *y = static_cast<const Real *>(b.state[t & 1][1]);
+    double tx = 0.0, ty = 0.0;
+    const long long need = (N + kThreads - 1) / kThreads;
+    const long long parts = need < kMonParts ? need : kMonParts;
+    for (long long p = 0; p < parts; ++p) {
+        double gx = 0.0, gy = 0.0;
+        for (long long i = p * kThreads + threadIdx.x; i < N; i += stride) {
+            const int32_t c = b.copy_from[i];
+            gx += (double)x[c];
+            gy += (double)y[c];
+        }
+        gx = warp_sum(gx);
+        gy = warp_sum(gy);
+        if ((threadIdx.x & 31) == 0) {
+            sh[0][threadIdx.x >> 5] = gx;
+            sh[1][threadIdx.x >> 5] = gy;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double px = 0.0, py = 0.0;
+            for (int w = 0; w < kThreads / 32; ++w) {
+                px += sh[0][w];
+                py += sh[1][w];
+            }
+            tx += px;
+            ty += py;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        b.hist_mean_x[t] = (anchored ? b.obs_x[t] : 0.0) + tx / (double)N;
+        b.hist_mean_y[t] = (anchored ? b.obs_y[t] : 0.0) + ty / (double)N;
+        b.ctl->monitor_done = t;
+    }
+}
+
+} // namespace vsmc_b200
+
+using namespace vsmc_b200;
+
+struct vsmc_cuda_cv_batch {
+    vsmc_cuda_cv_config model;
+    BatchConst bc;
+    cudaStream_t stream;
+    cudaMemPool_t pool;
+    uint32_t capacity;
+    uint64_t budget;
+    uint64_t in_use;
+    BatchSlot *d_slots;
+    std::vector<BatchSlot> slots; // host copies of the records
+    std::vector<char *> mem;      // per slot; nullptr = free
+    std::vector<uint64_t> bytes;
+    std::vector<uint64_t> t;      // steps enqueued
+    std::vector<uint64_t> T_obs;  // observations held
+    // work list: slot indices, tile offsets; pinned staging for both
+    int32_t *d_work;
+    int32_t *d_tile0;
+    int32_t *h_work;
+    TileRef *d_map;
+    size_t map_cap;
+    cudaEvent_t staged; // the last copy out of the pinned staging is done
+    // observations staging
+    ObsRecord *d_rec;
+    ObsRecord *h_rec;
+    double *d_obs;
+    size_t obs_cap;
+    double *h_obs; // pinned, 2 x capacity (append)
+    BatchSlot *h_slot; // pinned staging of one slot record
+    double *d_out;
+    double *h_out;
+    uint64_t launches;
+};
+
+namespace {
+
+bool is_residual(int s)
+{
+    return s == VSMC_CUDA_RESIDUAL || s == VSMC_CUDA_RESIDUAL_STRATIFIED ||
+           s == VSMC_CUDA_RESIDUAL_SYSTEMATIC;
+}
+
+bool is_sys(int s)
+{
+    return s == VSMC_CUDA_SYSTEMATIC || s == VSMC_CUDA_RESIDUAL_SYSTEMATIC;
+}
+
+bool is_strat(int s)
+{
+    return s == VSMC_CUDA_STRATIFIED || s == VSMC_CUDA_RESIDUAL_STRATIFIED;
+}
+
+size_t slot_bytes(const vsmc_cuda_cv_config &m, uint64_t N, uint64_t T)
+{
+    const size_t real = m.form == VSMC_CUDA_MIXED ? 4 : 8;
+    const size_t nt = (N + kTile - 1) / kTile;
+    size_t b = 0;
+    b += 8 * align256(N * real);                 // two state buffers
+    b += align256(N * real);                     // log-weights
+    b += align256(N * 4);                        // copy_from
+    b += align256(sizeof(FilterCtl));
+    b += align256(nt * sizeof(TileStats));
+    b += 2 * align256(T * 8);                    // observations
+    b += 4 * align256(T * 8) + align256(T * 4);  // histories
+    b += resample_workspace_bytes((long long)N);
+    return b;
+}
+
+void carve_slot(BatchSlot &s, char *p, const vsmc_cuda_cv_config &m,
+                uint64_t N, uint64_t T)
+{
+    const size_t real = m.form == VSMC_CUDA_MIXED ? 4 : 8;
+    const size_t nt = (N + kTile - 1) / kTile;
+    for (int b = 0; b < 2; ++b)
+        for (int d = 0; d < 4; ++d) {
+            s.state[b][d] = p;
+            p += align256(N * real);
+        }
+    s.lw = p;
+    p += align256(N * real);
+    s.copy_from = reinterpret_cast<int32_t *>(p);
+    p += align256(N * 4);
+    s.ctl = reinterpret_cast<FilterCtl *>(p);
+    p += align256(sizeof(FilterCtl));
+    s.tile_stats = reinterpret_cast<TileStats *>(p);
+    p += align256(nt * sizeof(TileStats));
+    s.obs_x = reinterpret_cast<double *>(p);
+    p += align256(T * 8);
+    s.obs_y = reinterpret_cast<double *>(p);
+    p += align256(T * 8);
+    s.hist_ess = reinterpret_cast<double *>(p);
+    p += align256(T * 8);
+    s.hist_logz_inc = reinterpret_cast<double *>(p);
+    p += align256(T * 8);
+    s.hist_mean_x = reinterpret_cast<double *>(p);
+    p += align256(T * 8);
+    s.hist_mean_y = reinterpret_cast<double *>(p);
+    p += align256(T * 8);
+    s.hist_resampled = reinterpret_cast<int32_t *>(p);
+    p += align256(T * 4);
+    s.rws = carve_workspace(p, (long long)N);
+    s.N = (long long)N;
+    s.T_max = (long long)T;
+    s.t = 0;
+    s.ntiles = (int)nt;
+}
+
+bool valid_slot(const vsmc_cuda_cv_batch *b, uint32_t s)
+{
+    return s < b->capacity && b->mem[s] != nullptr;
+}
+
+// Copies the work list into the device arrays: slots in the given order,
+// tile offsets as their exclusive prefix.  Returns the tile total.
+int stage_work(vsmc_cuda_cv_batch *b, const std::vector<uint32_t> &w,
+               long long *tiles)
+{
+    const int n = (int)w.size();
+    cudaError_t e = cudaEventSynchronize(b->staged);
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_cv_batch: staging");
+    long long acc = 0;
+    int32_t *hw = b->h_work;
+    int32_t *ht = b->h_work + b->capacity;
+    for (int k = 0; k < n; ++k) {
+        hw[k] = (int32_t)w[k];
+        ht[k] = (int32_t)acc;
+        acc += b->slots[w[k]].ntiles;
+    }
+    ht[n] = (int32_t)acc;
+    if (acc > 0x7FFFFFFFLL) {
+        set_last_error("vsmc_cuda_cv_batch: more than 2^31 tiles in a step");
+        return VSMC_CUDA_EINVAL;
+    }
+    if ((size_t)acc > b->map_cap) {
+        if (b->d_map != nullptr)
+            cudaFreeAsync(b->d_map, b->stream);
+        b->d_map = nullptr;
+        size_t cap = std::max<size_t>((size_t)acc, 2 * b->map_cap);
+        e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&b->d_map),
+                                    cap * sizeof(TileRef), b->pool,
+                                    b->stream);
+        if (e != cudaSuccess) {
+            b->map_cap = 0;
+            return cuda_status(e, "vsmc_cuda_cv_batch: tile map");
+        }
+        b->map_cap = cap;
+    }
+    e = cudaMemcpyAsync(b->d_work, hw, (size_t)n * 4, cudaMemcpyHostToDevice,
+                        b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_tile0, ht, (size_t)(n + 1) * 4,
+                            cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaEventRecord(b->staged, b->stream);
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_cv_batch: work list");
+    if (n > 0) {
+        kb_expand<<<n, 256, 0, b->stream>>>(b->d_slots, b->d_work,
+                                            b->d_tile0, n, b->d_map);
+        ++b->launches;
+    }
+    *tiles = acc;
+    return VSMC_CUDA_OK;
+}
+
+// One step of the first n work items (whose tiles are the first `tiles`
+// map entries).
+template <typename Real>
+void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles)
+{
+    cudaStream_t s = b->stream;
+    const int scheme = b->model.scheme;
+    const bool residual = is_residual(scheme), sys = is_sys(scheme),
+               strat = is_strat(scheme);
+    const unsigned nt = (unsigned)tiles;
+    const BatchSlot *sl = b->d_slots;
+    const TileRef *map = b->d_map;
+    const int32_t *work = b->d_work;
+    kb_move<Real><<<nt, kThreads, 0, s>>>(sl, map, b->bc.p);
+    kb_finalize<<<n, kFinalThreads, 0, s>>>(sl, work, b->bc);
+    int launches = 2;
+    if (residual) {
+        kb_tile_sums<Real, true><<<nt, kThreads, 0, s>>>(sl, map);
+        if (sys)
+            kb_spine_weights<true, true><<<n, kSpineThreads, 0, s>>>(sl,
+                                                                    work);
+        else
+            kb_spine_weights<true, false><<<n, kSpineThreads, 0, s>>>(sl,
+                                                                     work);
+        launches += 2;
+    }
+    if (strat) {
+        kb_uniforms_stratified<<<nt, kThreads, 0, s>>>(sl, map);
+        launches += 1;
+    } else if (!sys) {
+        kb_sorted_tile_sums<<<nt, kThreads, 0, s>>>(sl, map);
+        kb_sorted_spine<<<n, kSpineThreads, 0, s>>>(sl, work);
+        kb_sorted_uniforms<<<nt, kThreads, 0, s>>>(sl, map);
+        launches += 3;
+    }
+    if (residual && sys)
+        kb_invert<Real, true, true><<<nt, kThreads, 0, s>>>(sl, map);
+    else if (residual)
+        kb_invert<Real, true, false><<<nt, kThreads, 0, s>>>(sl, map);
+    else if (sys)
+        kb_invert<Real, false, true><<<nt, kThreads, 0, s>>>(sl, map);
+    else
+        kb_invert<Real, false, false><<<nt, kThreads, 0, s>>>(sl, map);
+    kb_zero_spine<<<n, kSpineThreads, 0, s>>>(sl, work);
+    kb_cfrp_fill<<<nt, kThreads, 0, s>>>(sl, map);
+    kb_step_done<<<(n + 255) / 256, 256, 0, s>>>(b->d_slots, b->d_work, n);
+    launches += 4;
+    b->launches += launches;
+}
+
+void launch_step_any(vsmc_cuda_cv_batch *b, int n, long long tiles)
+{
+    if (b->model.form == VSMC_CUDA_MIXED)
+        launch_batch_step<float>(b, n, tiles);
+    else
+        launch_batch_step<double>(b, n, tiles);
+}
+
+int check_slots(const vsmc_cuda_cv_batch *b, uint32_t n,
+                const uint32_t *slots, const char *what)
+{
+    if (b == nullptr || (n > 0 && slots == nullptr) || n > b->capacity) {
+        set_last_error(std::string(what) + ": invalid arguments");
+        return VSMC_CUDA_EINVAL;
+    }
+    std::vector<char> seen(b->capacity, 0);
+    for (uint32_t k = 0; k < n; ++k) {
+        if (!valid_slot(b, slots[k])) {
+            set_last_error(std::string(what) + ": slot " +
+                           std::to_string(slots[k]) + " is not admitted");
+            return VSMC_CUDA_EINVAL;
+        }
+        if (seen[slots[k]]) {
+            set_last_error(std::string(what) + ": slot " +
+                           std::to_string(slots[k]) + " listed twice");
+            return VSMC_CUDA_EINVAL;
+        }
+        seen[slots[k]] = 1;
+    }
+    return VSMC_CUDA_OK;
+}
+
+int grow_obs(vsmc_cuda_cv_batch *b, size_t values)
+{
+    if (values <= b->obs_cap)
+        return VSMC_CUDA_OK;
+    if (b->d_obs != nullptr)
+        cudaFreeAsync(b->d_obs, b->stream);
+    b->d_obs = nullptr;
+    const size_t cap = std::max(values, 2 * b->obs_cap);
+    cudaError_t e = cudaMallocFromPoolAsync(
+        reinterpret_cast<void **>(&b->d_obs), 2 * cap * sizeof(double),
+        b->pool, b->stream);
+    if (e != cudaSuccess) {
+        b->obs_cap = 0;
+        return cuda_status(e, "vsmc_cuda_cv_batch: observation staging");
+    }
+    b->obs_cap = cap;
+    return VSMC_CUDA_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+uint64_t vsmc_cuda_cv_batch_slot_bytes(const vsmc_cuda_cv_config *model,
+                                       uint64_t N, uint64_t T_max)
+{
+    if (model == nullptr || N < 2 || N > (1ull << 30) || T_max < 1 ||
+        T_max > (1ull << 31))
+        return 0;
+    return slot_bytes(*model, N, T_max);
+}
+
+int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
+                              uint32_t capacity, uint64_t hbm_budget,
+                              void *stream, vsmc_cuda_cv_batch **out)
+{
+    if (out == nullptr || model == nullptr || capacity == 0 ||
+        capacity > (1u << 24) || model->scheme < 0 || model->scheme > 5 ||
+        (model->form != VSMC_CUDA_FP64 && model->form != VSMC_CUDA_MIXED) ||
+        !(model->threshold >= 0.0)) {
+        set_last_error("vsmc_cuda_cv_batch_create: invalid arguments");
+        return VSMC_CUDA_EINVAL;
+    }
+    *out = nullptr;
+    vsmc_cuda_cv_batch *b = new (std::nothrow) vsmc_cuda_cv_batch();
+    if (b == nullptr)
+        return VSMC_CUDA_ENOMEM;
+    b->model = *model;
+    b->bc.p = cv_param(*model);
+    b->bc.threshold = model->threshold;
+    b->bc.residual = is_residual(model->scheme);
+    b->bc.sys = is_sys(model->scheme);
+    b->bc.anchored = model->form == VSMC_CUDA_MIXED;
+    b->stream = static_cast<cudaStream_t>(stream);
+    b->capacity = capacity;
+    b->budget = hbm_budget;
+    b->in_use = 0;
+    b->slots.resize(capacity);
+    b->mem.assign(capacity, nullptr);
+    b->bytes.assign(capacity, 0);
+    b->t.assign(capacity, 0);
+    b->T_obs.assign(capacity, 0);
+    b->d_map = nullptr;
+    b->map_cap = 0;
+    b->d_obs = nullptr;
+    b->obs_cap = 0;
+    b->launches = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    if (e == cudaSuccess)
+        e = cudaMemPoolCreate(&b->pool, &props);
+    if (e != cudaSuccess) {
+        delete b;
+        return cuda_status(e, "vsmc_cuda_cv_batch_create: memory pool");
+    }
+    // keep freed slots' memory in the pool for the next admissions
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    const size_t n = capacity;
+    e = cudaMalloc(&b->d_slots, n * sizeof(BatchSlot));
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->d_work, (2 * n + 1) * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->d_rec, n * sizeof(ObsRecord));
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->d_out, n * 5 * sizeof(double));
+    if (e == cudaSuccess)
+        e = cudaMallocHost(&b->h_work, (2 * n + 1) * 4);
+    if (e == cudaSuccess)
+        e = cudaMallocHost(&b->h_rec, n * sizeof(ObsRecord));
+    if (e == cudaSuccess)
+        e = cudaMallocHost(&b->h_obs, 2 * n * sizeof(double));
+    if (e == cudaSuccess)
+        e = cudaMallocHost(&b->h_out, n * 5 * sizeof(double));
+    if (e == cudaSuccess)
+        e = cudaMallocHost(&b->h_slot, sizeof(BatchSlot));
+    if (e == cudaSuccess)
+        e = cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_last_error("vsmc_cuda_cv_batch_create: allocation failed");
+        // partial allocations are released by destroy
+        vsmc_cuda_cv_batch_destroy(b);
+        return VSMC_CUDA_ENOMEM;
+    }
+    b->d_tile0 = b->d_work + n;
+    e = cudaMemsetAsync(b->d_slots, 0, n * sizeof(BatchSlot), b->stream);
+    if (e == cudaSuccess)
+        e = cudaEventRecord(b->staged, b->stream);
+    if (e != cudaSuccess) {
+        vsmc_cuda_cv_batch_destroy(b);
+        return cuda_status(e, "vsmc_cuda_cv_batch_create");
+    }
+    *out = b;
+    return VSMC_CUDA_OK;
+}
+
+int vsmc_cuda_cv_batch_destroy(vsmc_cuda_cv_batch *b)
+{
+    if (b == nullptr)
+        return VSMC_CUDA_OK;
+    cudaStreamSynchronize(b->stream);
+    for (char *m : b->mem)
+        if (m != nullptr)
+            cudaFreeAsync(m, b->stream);
+    if (b->d_map != nullptr)
+        cudaFreeAsync(b->d_map, b->stream);
+    if (b->d_obs != nullptr)
+        cudaFreeAsync(b->d_obs, b->stream);
+    cudaStreamSynchronize(b->stream);
+    cudaFree(b->d_slots);
+    cudaFree(b->d_work);
+    cudaFree(b->d_rec);
+    cudaFree(b->d_out);
+    cudaFreeHost(b->h_work);
+    cudaFreeHost(b->h_rec);
+    cudaFreeHost(b->h_obs);
+    cudaFreeHost(b->h_out);
+    cudaFreeHost(b->h_slot);
+    cudaEventDestroy(b->staged);
+    cudaMemPoolDestroy(b->pool);
+    cudaError_t e = cudaGetLastError();
+    delete b;
+    return e == cudaSuccess ? VSMC_CUDA_OK
+                            : cuda_status(e, "vsmc_cuda_cv_batch_destroy");
+}
+
+int vsmc_cuda_cv_batch_admit(vsmc_cuda_cv_batch *b, uint64_t N,
+                             uint64_t T_max, uint32_t seed,
+                             uint32_t stream_id, uint32_t *slot)
+{
+    if (b == nullptr || slot == nullptr || N < 2 || N > (1ull << 30) ||
+        T_max < 1 || T_max > (1ull << 31)) {
+        set_last_error("vsmc_cuda_cv_batch_admit: invalid arguments");
+        return VSMC_CUDA_EINVAL;
+    }
+    uint32_t s = 0;
+    while (s < b->capacity && b->mem[s] != nullptr)
+        ++s;
+    if (s == b->capacity) {
+        set_last_error("vsmc_cuda_cv_batch_admit: every slot is in use");
+        return VSMC_CUDA_ENOMEM;
+    }
+    const uint64_t bytes = slot_bytes(b->model, N, T_max);
+    if (b->budget != 0 && b->in_use + bytes > b->budget) {
+        set_last_error("vsmc_cuda_cv_batch_admit: " + std::to_string(bytes) +
+                       " bytes exceed the remaining budget of " +
+                       std::to_string(b->budget - b->in_use));
+        return VSMC_CUDA_ENOMEM;
+    }
+    char *m = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&m),
+                                            bytes, b->pool, b->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_last_error("vsmc_cuda_cv_batch_admit: device allocation of " +
+                       std::to_string(bytes) + " bytes failed");
+        return VSMC_CUDA_ENOMEM;
+    }
+    BatchSlot &r = b->slots[s];
+    std::memset(&r, 0, sizeof(r));
+    carve_slot(r, m, b->model, N, T_max);
+    r.eng = cv_resample_engine(seed);
+    r.k0 = cv_model_key(seed);
+    r.stream_id = stream_id;
+    e = cudaMemsetAsync(m, 0, bytes, b->stream);
+    if (e == cudaSuccess)
+        e = cudaEventSynchronize(b->staged);
+    if (e == cudaSuccess) {
+        // the record travels through the pinned staging
+        *b->h_slot = r;
+        e = cudaMemcpyAsync(b->d_slots + s, b->h_slot, sizeof(r),
+                            cudaMemcpyHostToDevice, b->stream);
+    }
+    if (e == cudaSuccess)
+        e = cudaEventRecord(b->staged, b->stream);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(m, b->stream);
+        return cuda_status(e, "vsmc_cuda_cv_batch_admit");
+    }
+    kb_reset_slot<<<1, 32, 0, b->stream>>>(b->d_slots, (int)s);
+    ++b->launches;
+    b->mem[s] = m;
+    b->bytes[s] = bytes;
+    b->in_use += bytes;
+    b->t[s] = 0;
+    b->T_obs[s] = 0;
+    *slot = s;
+    return VSMC_CUDA_OK;
+}
+
+int vsmc_cuda_cv_batch_release(vsmc_cuda_cv_batch *b, uint32_t slot)
+{
+    if (b == nullptr || !valid_slot(b, slot)) {
+        set_last_error("vsmc_cuda_cv_batch_release: slot not admitted");
+        return VSMC_CUDA_EINVAL;
+    }
+    cudaError_t e = cudaFreeAsync(b->mem[slot], b->stream);
+    b->mem[slot] = nullptr;
+    b->in_use -= b->bytes[slot];
+    b->bytes[slot] = 0;
+    return e == cudaSuccess ? VSMC_CUDA_OK
+                            : cuda_status(e, "vsmc_cuda_cv_batch_release");
+}
+
+int vsmc_cuda_cv_batch_bytes_in_use(vsmc_cuda_cv_batch *b, uint64_t *bytes)
+{
+    if (b == nullptr || bytes == nullptr)
+        return VSMC_CUDA_EINVAL;
+    *bytes = b->in_use;
+    return VSMC_CUDA_OK;
+}
+
+int vsmc_cuda_cv_batch_set_observations(vsmc_cuda_cv_batch *b, uint32_t n,
+                                        const uint32_t *slots,
+                                        const uint64_t *T, const double *ox,
+                                        const double *oy, int on_device)
+{
+    int st = check_slots(b, n, slots, "vsmc_cuda_cv_batch_set_observations");
+    if (st != VSMC_CUDA_OK)
+        return st;
+    if (n > 0 && (T == nullptr || ox == nullptr || oy == nullptr)) {
+        set_last_error("vsmc_cuda_cv_batch_set_observations: null array");
+        return VSMC_CUDA_EINVAL;
+    }
+    size_t total = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t s = slots[k];
+        if (T[k] == 0 || T[k] > (uint64_t)b->slots[s].T_max ||
+            T[k] > 0x7FFFFFFFull) {
+            set_last_error("vsmc_cuda_cv_batch_set_observations: slot " +
+                           std::to_string(s) + " series length invalid");
+            return VSMC_CUDA_EINVAL;
+        }
+        total += T[k];
+    }
+    if (n == 0)
+        return VSMC_CUDA_OK;
+    st = grow_obs(b, total);
+    if (st != VSMC_CUDA_OK)
+        return st;
+    cudaError_t e = cudaEventSynchronize(b->staged);
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_cv_batch_set_observations");
+    size_t off = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        ObsRecord r;
+        r.slot = (int32_t)slots[k];
+        r.count = (int32_t)T[k];
+        r.index = 0;
+        r.src = (long long)off;
+        b->h_rec[k] = r;
+        off += T[k];
+    }
+    const cudaMemcpyKind kind =
+        on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    e = cudaMemcpyAsync(b->d_obs, ox, total * 8, kind, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_obs + b->obs_cap, oy, total * 8, kind,
+                            b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_rec, b->h_rec, n * sizeof(ObsRecord),
+                            cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaEventRecord(b->staged, b->stream);
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_cv_batch_set_observations");
+    kb_scatter_obs<<<n, 256, 0, b->stream>>>(b->d_slots, b->d_rec, b->d_obs,
+                                             b->d_obs + b->obs_cap);
+    ++b->launches;
+    for (uint32_t k = 0; k < n; ++k)
+        b->T_obs[slots[k]] = T[k];
+    e = cudaGetLastError();
+    return e == cudaSuccess
+               ? VSMC_CUDA_OK
+               : cuda_status(e, "vsmc_cuda_cv_batch_set_observations");
+}
+
+int vsmc_cuda_cv_batch_append_observations(vsmc_cuda_cv_batch *b,
+                                           uint32_t n, const uint32_t *slots,
+                                           const double *x, const double *y)
+{
+    int st =
+        check_slots(b, n, slots, "vsmc_cuda_cv_batch_append_observations");
+    if (st != VSMC_CUDA_OK)
+        return st;
+    if (n == 0)
+        return VSMC_CUDA_OK;
+    if (x == nullptr || y == nullptr) {
+        set_last_error("vsmc_cuda_cv_batch_append_observations: null array");
+        return VSMC_CUDA_EINVAL;
+    }
+    for (uint32_t k = 0; k < n; ++k)
+        if (b->T_obs[slots[k]] >= (uint64_t)b->slots[slots[k]].T_max) {
+            set_last_error("vsmc_cuda_cv_batch_append_observations: slot " +
+                           std::to_string(slots[k]) + " is full");
+            return VSMC_CUDA_EINVAL;
+        }
+    cudaError_t e = cudaEventSynchronize(b->staged);
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_cv_batch_append_observations");
+    // pinned staging: records, then x values, then y values (in h_obs)
+    for (uint32_t k = 0; k < n; ++k) {
+        ObsRecord r;
+        r.slot = (int32_t)slots[k];
+        r.count = 1;
+        r.index = (long long)b->T_obs[slots[k]];
+        r.src = (long long)k;
+        b->h_rec[k] = r;
+        b->h_obs[k] = x[k];
+        b->h_obs[b->capacity + k] = y[k];
+    }
+    st = grow_obs(b, b->capacity);
+    if (st != VSMC_CUDA_OK)
+        return st;
+    e = cudaMemcpyAsync(b->d_rec, b->h_rec, n * sizeof(ObsRecord),
+                        cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_obs, b->h_obs, n * 8,
+                            cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_obs + b->obs_cap, b->h_obs + b->capacity,
+                            n * 8, cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaEventRecord(b->staged, b->stream);
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_cv_batch_append_observations");
+    kb_scatter_obs<<<n, 32, 0, b->stream>>>(b->d_slots, b->d_rec, b->d_obs,
+                                            b->d_obs + b->obs_cap);
+    ++b->launches;
+    for (uint32_t k = 0; k < n; ++k)
+        ++b->T_obs[slots[k]];
+    e = cudaGetLastError();
+    return e == cudaSuccess
+               ? VSMC_CUDA_OK
+               : cuda_status(e, "vsmc_cuda_cv_batch_append_observations");
+}
+
+int vsmc_cuda_cv_batch_initialize(vsmc_cuda_cv_batch *b, uint32_t n,
+                                  const uint32_t *slots)
+{
+    int st = check_slots(b, n, slots, "vsmc_cuda_cv_batch_initialize");
+    if (st != VSMC_CUDA_OK)
+        return st;
+    if (n == 0)
+        return VSMC_CUDA_OK;
+    std::vector<uint32_t> w(slots, slots + n);
+    long long tiles = 0;
+    st = stage_work(b, w, &tiles);
+    if (st != VSMC_CUDA_OK)
+        return st;
+    kb_reset<<<(n + 255) / 256, 256, 0, b->stream>>>(b->d_slots, b->d_work,
+                                                    (int)n);
+    ++b->launches;
+    for (uint32_t k = 0; k < n; ++k)
+        b->t[slots[k]] = 0;
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VSMC_CUDA_OK
+                            : cuda_status(e, "vsmc_cuda_cv_batch_initialize");
+}
+
+int vsmc_cuda_cv_batch_step(vsmc_cuda_cv_batch *b, uint32_t n,
+                            const uint32_t *slots)
+{
+    int st = check_slots(b, n, slots, "vsmc_cuda_cv_batch_step");
+    if (st != VSMC_CUDA_OK)
+        return st;
+    for (uint32_t k = 0; k < n; ++k)
+        if (b->t[slots[k]] >= b->T_obs[slots[k]]) {
+            set_last_error("vsmc_cuda_cv_batch_step: slot " +
+                           std::to_string(slots[k]) +
+                           " has no observation for its next step");
+            return VSMC_CUDA_EINVAL;
+        }
+    if (n == 0)
+        return VSMC_CUDA_OK;
+    std::vector<uint32_t> w(slots, slots + n);
+    long long tiles = 0;
+    st = stage_work(b, w, &tiles);
+    if (st != VSMC_CUDA_OK)
+        return st;
+    launch_step_any(b, (int)n, tiles);
+    for (uint32_t k = 0; k < n; ++k)
+        ++b->t[slots[k]];
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VSMC_CUDA_OK
+                            : cuda_status(e, "vsmc_cuda_cv_batch_step");
+}
+
+int vsmc_cuda_cv_batch_run(vsmc_cuda_cv_batch *b, uint32_t n,
+                           const uint32_t *slots)
+{
+    int st = check_slots(b, n, slots, "vsmc_cuda_cv_batch_run");
+    if (st != VSMC_CUDA_OK)
+        return st;
+    if (n == 0)
+        return VSMC_CUDA_OK;
+    // longest remaining series first: the slots still running at step k
+    // are a prefix of the list, and so are their tiles
+    std::vector<uint32_t> w(slots, slots + n);
+    std::stable_sort(w.begin(), w.end(), [b](uint32_t a, uint32_t c) {
+        return b->T_obs[a] - b->t[a] > b->T_obs[c] - b->t[c];
+    });
+    long long tiles = 0;
+    st = stage_work(b, w, &tiles);
+    if (st != VSMC_CUDA_OK)
+        return st;
+    std::vector<long long> tile0(n + 1, 0);
+    for (uint32_t k = 0; k < n; ++k)
+        tile0[k + 1] = tile0[k] + b->slots[w[k]].ntiles;
+    int active = (int)n;
+    for (uint64_t step = 0;; ++step) {
+        while (active > 0 &&
+               b->T_obs[w[active - 1]] - b->t[w[active - 1]] <= step)
+            --active;
+        if (active == 0)
+            break;
+        launch_step_any(b, active, tile0[active]);
+    }
+    for (uint32_t k = 0; k < n; ++k)
+        b->t[slots[k]] = b->T_obs[slots[k]];
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VSMC_CUDA_OK
+                            : cuda_status(e, "vsmc_cuda_cv_batch_run");
+}
+
+int vsmc_cuda_cv_batch_read_last(vsmc_cuda_cv_batch *b, uint32_t n,
+                                 const uint32_t *slots, double *ess,
+                                 double *logz_inc, int32_t *resampled,
+                                 double *log_evidence)
+{
+    int st = check_slots(b, n, slots, "vsmc_cuda_cv_batch_read_last");
+    if (st != VSMC_CUDA_OK)
+        return st;
+    if (n == 0)
+        return VSMC_CUDA_OK;
+    std::vector<uint32_t> w(slots, slots + n);
+    long long tiles = 0;
+    st = stage_work(b, w, &tiles);
+    if (st != VSMC_CUDA_OK)
+        return st;
+    kb_read_last<<<(n + 255) / 256, 256, 0, b->stream>>>(
+        b->d_slots, b->d_work, (int)n, b->d_out);
+    ++b->launches;
+    cudaError_t e = cudaMemcpyAsync(b->h_out, b->d_out, n * 5 * 8,
+                                    cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_cv_batch_read_last");
+    int err = VSMC_CUDA_OK;
+    for (uint32_t k = 0; k < n; ++k) {
+        const double *o = b->h_out + 5 * k;
+        if (ess)
+            ess[k] = o[0];
+        if (logz_inc)
+            logz_inc[k] = o[1];
+        if (resampled)
+            resampled[k] = (int32_t)o[2];
+        if (log_evidence)
+            log_evidence[k] = o[3];
+        if (o[4] != 0.0 && err == VSMC_CUDA_OK)
+            err = (int)o[4];
+    }
+    if (err != VSMC_CUDA_OK)
+        set_last_error(err == VSMC_CUDA_EDEGENERATE
+                           ? "vsmc_cuda_cv_batch: degenerate weights in a "
+                             "listed slot"
+                           : "vsmc_cuda_cv_batch: device error in a listed "
+                             "slot");
+    return err;
+}
+
+int vsmc_cuda_cv_batch_iter_size(vsmc_cuda_cv_batch *b, uint32_t slot,
+                                 uint64_t *n)
+{
+    if (b == nullptr || n == nullptr || !valid_slot(b, slot))
+        return VSMC_CUDA_EINVAL;
+    *n = b->t[slot];
+    return VSMC_CUDA_OK;
+}
+
+int vsmc_cuda_cv_batch_history(vsmc_cuda_cv_batch *b, uint32_t slot,
+                               double *ess, int32_t *resampled,
+                               double *logz_inc, double *mean_x,
+                               double *mean_y)
+{
+    if (b == nullptr || !valid_slot(b, slot)) {
+        set_last_error("vsmc_cuda_cv_batch_history: slot not admitted");
+        return VSMC_CUDA_EINVAL;
+    }
+    const uint64_t T = b->t[slot];
+    if (T == 0)
+        return VSMC_CUDA_OK;
+    std::vector<uint32_t> w(1, slot);
+    long long tiles = 0;
+    int st = stage_work(b, w, &tiles);
+    if (st != VSMC_CUDA_OK)
+        return st;
+    if (b->model.form == VSMC_CUDA_MIXED)
+        kb_monitor_flush<float><<<1, kThreads, 0, b->stream>>>(
+            b->d_slots, b->d_work, 1);
+    else
+        kb_monitor_flush<double><<<1, kThreads, 0, b->stream>>>(
+            b->d_slots, b->d_work, 0);
+    ++b->launches;
+    const BatchSlot &r = b->slots[slot];
+    cudaError_t e = cudaSuccess;
+    auto get = [&](void *dst, const void *src, size_t bytes) {
+        if (dst != nullptr && e == cudaSuccess)
+            e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost,
+                                b->stream);
+    };
+    get(ess, r.hist_ess, T * 8);
+    get(resampled, r.hist_resampled, T * 4);
+    get(logz_inc, r.hist_logz_inc, T * 8);
+    get(mean_x, r.hist_mean_x, T * 8);
+    get(mean_y, r.hist_mean_y, T * 8);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(b->stream);
+    return e == cudaSuccess ? VSMC_CUDA_OK
+                            : cuda_status(e, "vsmc_cuda_cv_batch_history");
+}
+
+int vsmc_cuda_cv_batch_synchronize(vsmc_cuda_cv_batch *b)
+{
+    if (b == nullptr)
+        return VSMC_CUDA_EINVAL;
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    return e == cudaSuccess ? VSMC_CUDA_OK
+                            : cuda_status(e, "vsmc_cuda_cv_batch_synchronize");
+}
+
+int vsmc_cuda_cv_batch_launches(vsmc_cuda_cv_batch *b, uint64_t *launches)
+{
+    if (b == nullptr || launches == nullptr)
+        return VSMC_CUDA_EINVAL;
+    *launches = b->launches;
+    return VSMC_CUDA_OK;
+}
+
+} // extern "C"

@@ -150,19 +150,50 @@ __device__ __forceinline__ double residual_split(double w, double Nd,
     return modf(__dmul_rn(Nd, w), &k);
 }
 
+// Shared memory of each per-tile body (the __global__ wrappers declare one;
+// a caller that runs several bodies in one CTA can overlay them).
+struct SmemTileSums {
+    double shd[kThreads / 32];
+    long long shk[kThreads / 32];
+};
+struct SmemSpine {
+    double shd[kSpineThreads / 32];
+    long long shk[kSpineThreads / 32];
+    double coeff;
+};
+struct SmemNone {
+    int unused;
+};
+struct SmemSortedSums {
+    double sh[kThreads / 32];
+};
+struct SmemSortedUniforms {
+    double sh[kThreads / 32];
+    double shm[kThreads];
+};
+template <bool Residual>
+struct SmemInvert {
+    double sw[kTile];                // weights, then uniforms
+    double sk[Residual ? kTile : 1]; // floor(N w) (residual)
+    long long shl[kThreads / 32];
+    double shd[kThreads / 32];
+    long long bound[2];
+    long long last[kThreads / 32];
+};
+
 // ---------------------------------------------------------------------------
 // Tile sums of the weights (or, residual, of r and k).
 template <typename W, bool Residual>
-__global__ void __launch_bounds__(kThreads)
-k_tile_sums(W wsrc, long long N, const ResampleCtl *ctl, double *tile_sum,
-            long long *tile_k)
+__device__ __forceinline__ void
+k_tile_sums_body(W wsrc, long long N, const ResampleCtl *ctl, double *tile_sum,
+                 long long *tile_k, int bid, SmemTileSums &sm)
 {
     if (!ctl->active)
         return;
-    __shared__ double shd[kThreads / 32];
-    __shared__ long long shk[kThreads / 32];
+    double *shd = sm.shd;
+    long long *shk = sm.shk;
     wsrc.prepare();
-    const long long base = (long long)blockIdx.x * kTile;
+    const long long base = (long long)bid * kTile;
     const double Nd = (double)N;
     double s = 0.0;
     long long ks = 0;
@@ -195,10 +226,20 @@ k_tile_sums(W wsrc, long long N, const ResampleCtl *ctl, double *tile_sum,
             t += shd[w];
             kt += shk[w];
         }
-        tile_sum[blockIdx.x] = t;
+        tile_sum[bid] = t;
         if (Residual)
-            tile_k[blockIdx.x] = kt;
+            tile_k[bid] = kt;
     }
+}
+
+template <typename W, bool Residual>
+__global__ void __launch_bounds__(kThreads)
+k_tile_sums(W wsrc, long long N, const ResampleCtl *ctl, double *tile_sum,
+            long long *tile_k)
+{
+    __shared__ SmemTileSums sm;
+    k_tile_sums_body<W, Residual>(wsrc, N, ctl, tile_sum, tile_k, blockIdx.x,
+        sm);
 }
 
 // One CTA: exclusive prefix of `ntiles` doubles in a fixed association
@@ -250,16 +291,17 @@ __device__ __forceinline__ void spine_scan_ll(const long long *in,
 // systematic start u0 (one engine word, U01SequenceSystematic's constructor,
 // u01.hpp:253-263) and the words drawn when they do not depend on the data.
 template <bool Residual, bool Sys>
-__global__ void __launch_bounds__(kSpineThreads)
-k_spine_weights(const double *tile_sum, const long long *tile_k,
-                double *tile_excl, long long *tile_kexcl, int ntiles,
-                long long N, EngineRef eng, ResampleCtl *ctl)
+__device__ __forceinline__ void
+k_spine_weights_body(const double *tile_sum, const long long *tile_k,
+                     double *tile_excl, long long *tile_kexcl, int ntiles,
+                     long long N, EngineRef eng, ResampleCtl *ctl, int bid,
+                     SmemSpine &sm)
 {
     if (!ctl->active)
         return;
-    __shared__ double shd[kSpineThreads / 32];
-    __shared__ long long shk[kSpineThreads / 32];
-    __shared__ double coeff_sh;
+    double *shd = sm.shd;
+    long long *shk = sm.shk;
+    double &coeff_sh = sm.coeff;
     long long NN = N;
     double coeff = 1.0;
     if (Residual) {
@@ -268,7 +310,8 @@ k_spine_weights(const double *tile_sum, const long long *tile_k,
         // asum of the residuals in the spine's fixed order
         const int per = (ntiles + blockDim.x - 1) / blockDim.x;
         double run = 0.0;
-        for (int t = threadIdx.x * per; t < min((int)(threadIdx.x + 1) * per, ntiles); ++t)
+        const int e = min((int)(threadIdx.x + 1) * per, ntiles);
+        for (int t = threadIdx.x * per; t < e; ++t)
             run += tile_sum[t];
         double total;
         block_excl_scan(run, shd, total);
@@ -293,6 +336,17 @@ k_spine_weights(const double *tile_sum, const long long *tile_k,
             ctl->words = 0;
         }
     }
+}
+
+template <bool Residual, bool Sys>
+__global__ void __launch_bounds__(kSpineThreads)
+k_spine_weights(const double *tile_sum, const long long *tile_k,
+                double *tile_excl, long long *tile_kexcl, int ntiles,
+                long long N, EngineRef eng, ResampleCtl *ctl)
+{
+    __shared__ SmemSpine sm;
+    k_spine_weights_body<Residual, Sys>(tile_sum, tile_k, tile_excl, tile_kexcl,
+        ntiles, N, eng, ctl, blockIdx.x, sm);
 }
 
 // Words at stream positions pos0 .. pos0+7 of a Threefry4x64 engine (two or
@@ -329,9 +383,9 @@ __device__ __forceinline__ double strat_u(uint64_t w, long long n, double delta)
                      __dmul_rn((double)n, delta));
 }
 
-static __global__ void __launch_bounds__(kThreads)
-k_uniforms_stratified(EngineRef eng, const ResampleCtl *ctl, double *u,
-                      int32_t *L)
+__device__ __forceinline__ void
+k_uniforms_stratified_body(EngineRef eng, const ResampleCtl *ctl, double *u,
+                           int32_t *L, unsigned long long gid, SmemNone &sm)
 {
     if (!ctl->active)
         return;
@@ -340,7 +394,7 @@ k_uniforms_stratified(EngineRef eng, const ResampleCtl *ctl, double *u,
     const int kb = ctl->kbits;
     const unsigned long long off = ctl->offset;
     const unsigned long long b =
-        off / 4 + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+        off / 4 + (unsigned long long)gid;
     const bool live = b * 4 < off + (unsigned long long)NN;
     double raw[4] = {-INFINITY, -INFINITY, -INFINITY, -INFINITY};
     if (live) {
@@ -382,6 +436,15 @@ k_uniforms_stratified(EngineRef eng, const ResampleCtl *ctl, double *u,
     }
 }
 
+static __global__ void __launch_bounds__(kThreads)
+k_uniforms_stratified(EngineRef eng, const ResampleCtl *ctl, double *u,
+                      int32_t *L)
+{
+    __shared__ SmemNone sm;
+    k_uniforms_stratified_body(eng, ctl, u, L,
+        (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x, sm);
+}
+
 // Sorted U01 sequence (U01SequenceSorted, u01.hpp:165-202): lmax_n =
 // sum_{k<=n} log(1 - U_k) / (NN - k); u_n = 1 - exp(lmax_n).  Two passes
 // over tiles of kTile uniforms around a deterministic spine; each thread owns
@@ -404,15 +467,15 @@ __device__ __forceinline__ void sorted_terms8(const EngineRef &eng,
 
 // Pass 1: the terms log(1 - U_n) / (NN - n), stored in u[] for pass 2,
 // and their tile sums.
-static __global__ void __launch_bounds__(kThreads)
-k_sorted_tile_sums(EngineRef eng, const ResampleCtl *ctl, double *tile_sum,
-                   double *u)
+__device__ __forceinline__ void
+k_sorted_tile_sums_body(EngineRef eng, const ResampleCtl *ctl, double *tile_sum,
+                        double *u, int bid, SmemSortedSums &sm)
 {
     if (!ctl->active)
         return;
-    __shared__ double sh[kThreads / 32];
+    double *sh = sm.sh;
     const long long NN = ctl->NN;
-    const long long base = (long long)blockIdx.x * kTile;
+    const long long base = (long long)bid * kTile;
     if (base >= NN)
         return;
     double t[kItems];
@@ -428,30 +491,47 @@ k_sorted_tile_sums(EngineRef eng, const ResampleCtl *ctl, double *tile_sum,
     double total;
     block_excl_scan(s, sh, total);
     if (threadIdx.x == 0)
-        tile_sum[blockIdx.x] = total;
+        tile_sum[bid] = total;
+}
+
+static __global__ void __launch_bounds__(kThreads)
+k_sorted_tile_sums(EngineRef eng, const ResampleCtl *ctl, double *tile_sum,
+                   double *u)
+{
+    __shared__ SmemSortedSums sm;
+    k_sorted_tile_sums_body(eng, ctl, tile_sum, u, blockIdx.x, sm);
+}
+
+__device__ __forceinline__ void
+k_sorted_spine_body(const double *tile_sum, double *tile_excl,
+                    const ResampleCtl *ctl, int bid, SmemSpine &sm)
+{
+    if (!ctl->active)
+        return;
+    double *sh = sm.shd;
+    const int ntiles = (int)((ctl->NN + kTile - 1) / kTile);
+    spine_scan_f64(tile_sum, tile_excl, ntiles, 1.0, sh);
 }
 
 static __global__ void __launch_bounds__(kSpineThreads)
 k_sorted_spine(const double *tile_sum, double *tile_excl,
                const ResampleCtl *ctl)
 {
-    if (!ctl->active)
-        return;
-    __shared__ double sh[kSpineThreads / 32];
-    const int ntiles = (int)((ctl->NN + kTile - 1) / kTile);
-    spine_scan_f64(tile_sum, tile_excl, ntiles, 1.0, sh);
+    __shared__ SmemSpine sm;
+    k_sorted_spine_body(tile_sum, tile_excl, ctl, blockIdx.x, sm);
 }
 
-static __global__ void __launch_bounds__(kThreads)
-k_sorted_uniforms(EngineRef eng, const ResampleCtl *ctl,
-                  const double *tile_excl, double *u, int32_t *L)
+__device__ __forceinline__ void
+k_sorted_uniforms_body(EngineRef eng, const ResampleCtl *ctl,
+                       const double *tile_excl, double *u, int32_t *L, int bid,
+                       SmemSortedUniforms &sm)
 {
     if (!ctl->active)
         return;
-    __shared__ double sh[kThreads / 32];
-    __shared__ double shm[kThreads];
+    double *sh = sm.sh;
+    double *shm = sm.shm;
     const long long NN = ctl->NN;
-    const long long base = (long long)blockIdx.x * kTile;
+    const long long base = (long long)bid * kTile;
     if (base >= NN)
         return;
     const long long last = min(base + (long long)kTile, NN) - 1;
@@ -466,10 +546,10 @@ k_sorted_uniforms(EngineRef eng, const ResampleCtl *ctl,
         run += t[j];
     double total;
     double pre = block_excl_scan(run, sh, total);
-    const double a = tile_excl[blockIdx.x];
-    const double b = tile_excl[blockIdx.x + 1];
+    const double a = tile_excl[bid];
+    const double b = tile_excl[bid + 1];
     // carry: the previous tile ends exactly at lmax = a
-    const double umax = blockIdx.x > 0 ? __dadd_rn(1.0, -exp(a)) : -INFINITY;
+    const double umax = bid > 0 ? __dadd_rn(1.0, -exp(a)) : -INFINITY;
     double uv[kItems];
     double tmax = -INFINITY;
 #pragma unroll
@@ -504,6 +584,14 @@ k_sorted_uniforms(EngineRef eng, const ResampleCtl *ctl,
     }
 }
 
+static __global__ void __launch_bounds__(kThreads)
+k_sorted_uniforms(EngineRef eng, const ResampleCtl *ctl,
+                  const double *tile_excl, double *u, int32_t *L)
+{
+    __shared__ SmemSortedUniforms sm;
+    k_sorted_uniforms_body(eng, ctl, tile_excl, u, L, blockIdx.x, sm);
+}
+
 // ---------------------------------------------------------------------------
 // Count of the U01 sequence values <= C ("first n with u_n > C", which for a
 // non-decreasing sequence is the upper bound).
@@ -518,6 +606,22 @@ __device__ __forceinline__ int ub_shared(const double *u, int lo, int hi,
             hi = mid;
     }
     return lo;
+}
+
+// First index with s[index] > r in a non-decreasing int array of length n
+// (n - 1 when none is; callers check s[n - 1] > r first).
+__device__ __forceinline__ int first_above_shared(const int32_t *s, int n,
+                                                  long long r)
+{
+    int l = 0, h = n - 1;
+    while (l < h) {
+        const int m = (l + h) >> 1;
+        if (s[m] > r)
+            h = m;
+        else
+            l = m + 1;
+    }
+    return l;
 }
 
 __device__ __forceinline__ long long ub_global(const double *u, long long lo,
@@ -596,23 +700,24 @@ constexpr int kUStage = kTile; // uniforms staged in shared memory per tile
 // slot without offspring), sinc_local (surplus children of particles <= i
 // minus the zero slots of earlier tiles) and the tile's zero-slot count.
 template <typename W, bool Residual, bool Sys>
-__global__ void __launch_bounds__(kThreads)
-k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
-         const long long *tile_kexcl, const double *u, long long n_u,
-         const int32_t *L, int32_t *rep_out, int32_t *copy_from,
-         int32_t *sinc_local, int32_t *tile_zeros, int32_t *tile_sinc_last)
+__device__ __forceinline__ void
+k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
+              const long long *tile_kexcl, const double *u, long long n_u,
+              const int32_t *L, int32_t *rep_out, int32_t *copy_from,
+              int32_t *sinc_local, int32_t *tile_zeros, int32_t *tile_sinc_last,
+              int tile_bid, SmemInvert<Residual> &sm)
 {
     if (!ctl->active)
         return;
-    __shared__ double sw[kTile];                // weights, then uniforms
-    __shared__ double sk[Residual ? kTile : 1]; // floor(N w) (residual)
-    __shared__ long long shl[kThreads / 32];
-    __shared__ double shd[kThreads / 32];
-    __shared__ long long sh_bound[2];
-    __shared__ long long sh_last[kThreads / 32];
+    double *sw = sm.sw; // weights, then uniforms
+    double *sk = sm.sk; // floor(N w) (residual)
+    long long *shl = sm.shl;
+    double *shd = sm.shd;
+    long long *sh_bound = sm.bound;
+    long long *sh_last = sm.last;
     wsrc.prepare();
 
-    const int tile = blockIdx.x;
+    const int tile = tile_bid;
     const long long base = (long long)tile * kTile;
     const long long NN = ctl->NN;
     const double Nd = (double)N;
@@ -791,6 +896,19 @@ k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     }
 }
 
+template <typename W, bool Residual, bool Sys>
+__global__ void __launch_bounds__(kThreads)
+k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
+         const long long *tile_kexcl, const double *u, long long n_u,
+         const int32_t *L, int32_t *rep_out, int32_t *copy_from,
+         int32_t *sinc_local, int32_t *tile_zeros, int32_t *tile_sinc_last)
+{
+    __shared__ SmemInvert<Residual> sm;
+    k_invert_body<W, Residual, Sys>(wsrc, N, ctl, tile_excl, tile_kexcl, u, n_u,
+        L, rep_out, copy_from, sinc_local, tile_zeros, tile_sinc_last,
+        blockIdx.x, sm);
+}
+
 // Exclusive prefix of the per-tile zero-slot counts (one CTA) and, per
 // tile, the range of tiles holding the parents of its zero slots.  The
 // surplus count at the end of tile t is E[t] = tile_sinc_last[t] + zexcl[t]
@@ -798,15 +916,23 @@ k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
 // E > k, found by a binary search over E staged in shared memory.
 constexpr int kSpineStage = 8192; // tiles whose E fits in shared memory
 
-static __global__ void __launch_bounds__(kSpineThreads)
-k_zero_spine(const int32_t *tile_zeros, const int32_t *tile_sinc_last,
-             int32_t *zexcl, int32_t *tfirst, int32_t *tlast, int ntiles,
-             const ResampleCtl *ctl)
+struct SmemZeroSpine {
+    long long sh[kSpineThreads / 32];
+    int32_t S[kSpineStage]; // zero counts, then surplus ends E
+};
+struct SmemFill {
+    int32_t ss[kTile];
+};
+
+__device__ __forceinline__ void
+k_zero_spine_body(const int32_t *tile_zeros, const int32_t *tile_sinc_last,
+                  int32_t *zexcl, int32_t *tfirst, int32_t *tlast, int ntiles,
+                  const ResampleCtl *ctl, int bid, SmemZeroSpine &sm)
 {
     if (!ctl->active)
         return;
-    __shared__ long long sh[kSpineThreads / 32];
-    __shared__ int32_t S[kSpineStage]; // zero counts, then surplus ends E
+    long long *sh = sm.sh;
+    int32_t *S = sm.S; // zero counts, then surplus ends E
     const bool staged = ntiles <= kSpineStage;
     // phase 1: exclusive prefix of the zero counts (striped load, ordered
     // contiguous runs from shared memory)
@@ -867,20 +993,31 @@ k_zero_spine(const int32_t *tile_zeros, const int32_t *tile_sinc_last,
     }
 }
 
+static __global__ void __launch_bounds__(kSpineThreads)
+k_zero_spine(const int32_t *tile_zeros, const int32_t *tile_sinc_last,
+             int32_t *zexcl, int32_t *tfirst, int32_t *tlast, int ntiles,
+             const ResampleCtl *ctl)
+{
+    __shared__ SmemZeroSpine sm;
+    k_zero_spine_body(tile_zeros, tile_sinc_last, zexcl, tfirst, tlast, ntiles,
+        ctl, blockIdx.x, sm);
+}
+
 // internal::cfrp_trans for the slots without offspring (common.hpp:94-106):
 // the k-th such slot takes the k-th surplus child in parent order, i.e. the
 // first parent p with sinc(p) > k, sinc(p) = sinc_local[p] + zexcl[tile(p)].
 // The CTA of tile t stages the parent tiles tfirst[t]..tlast[t] one at a
 // time in shared memory; every slot binary-searches its parent there.
-static __global__ void __launch_bounds__(kThreads)
-k_cfrp_fill(long long N, ResampleCtl *ctl, const int32_t *sinc_local,
-            const int32_t *zexcl, const int32_t *tfirst, const int32_t *tlast,
-            int32_t *copy_from)
+__device__ __forceinline__ void
+k_cfrp_fill_body(long long N, ResampleCtl *ctl, const int32_t *sinc_local,
+                 const int32_t *zexcl, const int32_t *tfirst,
+                 const int32_t *tlast, int32_t *copy_from, int tile_bid,
+                 SmemFill &sm)
 {
     if (!ctl->active)
         return;
-    __shared__ int32_t ss[kTile];
-    const int tile = blockIdx.x;
+    int32_t *ss = sm.ss;
+    const int tile = tile_bid;
     const int t0 = tfirst[tile], t1 = tlast[tile];
     if (t1 < t0)
         return; // every particle of the tile has offspring
@@ -910,15 +1047,8 @@ k_cfrp_fill(long long N, ResampleCtl *ctl, const int32_t *sinc_local,
 #pragma unroll
         for (int j = 0; j < kItems; ++j) {
             if (rank[j] >= 0 && rank[j] < top) {
-                int l = 0, h = len - 1; // first index with ss > rank
-                while (l < h) {
-                    const int m = (l + h) >> 1;
-                    if (ss[m] > rank[j])
-                        h = m;
-                    else
-                        l = m + 1;
-                }
-                parent[j] = (int32_t)(pb + l);
+                parent[j] =
+                    (int32_t)(pb + first_above_shared(ss, len, rank[j]));
                 rank[j] = -2;
             }
         }
@@ -934,6 +1064,16 @@ k_cfrp_fill(long long N, ResampleCtl *ctl, const int32_t *sinc_local,
             copy_from[i] = (int32_t)i;
         }
     }
+}
+
+static __global__ void __launch_bounds__(kThreads)
+k_cfrp_fill(long long N, ResampleCtl *ctl, const int32_t *sinc_local,
+            const int32_t *zexcl, const int32_t *tfirst, const int32_t *tlast,
+            int32_t *copy_from)
+{
+    __shared__ SmemFill sm;
+    k_cfrp_fill_body(N, ctl, sinc_local, zexcl, tfirst, tlast, copy_from,
+        blockIdx.x, sm);
 }
 
 // Finalise the engine position.
