@@ -149,6 +149,176 @@ def cpu_reference(N, scheme, warmup, steps, sample_steps=None):
                                              "steps": n_steps}
 
 
+def forms_compare(capi, N, sch, K, W, ox, oy, sp, fp64_step_ms):
+    """Mixed form (float move / weights, double scan and log-evidence) against
+    the FP64 form on the same inputs: device step time, and the relative
+    log-evidence error on the FP64 run's ancestry (the mixed run replays the
+    FP64 run's resampling decisions and copy_from vectors)."""
+    import torch
+
+    T = 1 + W + K
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.ExternalStream(sp)
+    with capi.CVFilter(N, T, scheme=sch, form=capi.MIXED, seed=101, stream=sp) as m:
+        m.set_observations_host(ox, oy)
+        m.initialize()
+        m.iterate(W)
+        m.synchronize()
+        e0.record(stream)
+        m.iterate(K)
+        e1.record(stream)
+        m.synchronize()
+        torch.cuda.synchronize()
+        mixed_ms = e0.elapsed_time(e1) / K
+        m.initialize()
+        m.iterate(W)
+        m.set_timing(True)
+        m.iterate(K)
+        mv_ms, st_ms, n, _ = m.timing()
+    # fixed ancestry: record the FP64 run, replay it in the mixed form
+    rec = torch.empty(T * N, dtype=torch.int32, device="cuda")
+    with capi.CVFilter(N, T, scheme=sch, form=capi.FP64, seed=101, stream=sp) as f:
+        f.set_observations_host(ox, oy)
+        f.set_ancestry(record_ptr=rec.data_ptr())
+        f.initialize()
+        f.iterate(T - 1)
+        h64 = f.history()
+        z64 = f.log_evidence()
+    flags = torch.from_numpy(h64["resampled"].astype("int32")).cuda()
+    with capi.CVFilter(N, T, scheme=sch, form=capi.MIXED, seed=101, stream=sp) as m:
+        m.set_observations_host(ox, oy)
+        m.set_ancestry(replay_ptr=rec.data_ptr(), replay_flags_ptr=flags.data_ptr())
+        m.initialize()
+        m.iterate(T - 1)
+        z32 = m.log_evidence()
+    del rec
+    torch.cuda.synchronize()
+    return {"mixed_value": N / (mixed_ms / 1e3), "mixed_ms_per_step": mixed_ms,
+            "fp64_ms_per_step": fp64_step_ms, "speedup_mixed_vs_fp64": fp64_step_ms / mixed_ms,
+            "mixed_move_ms": mv_ms / n, "log_evidence_fp64": z64, "log_evidence_mixed": z32,
+            "rel_log_evidence_error": abs(z32 - z64) / abs(z64),
+            "error_method": "mixed run replays the FP64 run's resampling decisions and "
+                            "copy_from vectors (fixed ancestry) over the same T steps"}
+
+
+def batched_workload(capi, n_filters=4096, seed=2024):
+    """4096 filters: N log-uniform on [2^10, 2^16], T uniform on [50, 500],
+    each with its own simulated series (obs seed 1000 + k, stream k)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    N = np.exp(rng.uniform(np.log(2 ** 10), np.log(2 ** 16), n_filters)).astype(np.int64)
+    T = rng.integers(50, 501, n_filters)
+    obs = [capi.cv_simulate(int(T[k]), obs_seed=1000 + k, stream_id=k)
+           for k in range(n_filters)]
+    return N, T, obs
+
+
+def batched_run(capi, form, N, T, obs, reps=3):
+    """Every filter run to the end of its series in one batch: the run is
+    one CUDA graph (a step = one launch per kernel over all live filters'
+    tiles).  Device time with CUDA events; e2e adds the observation upload
+    from host memory and the log-evidence read back."""
+    import numpy as np
+    import torch
+
+    nf = len(N)
+    psteps = float(np.sum(N * T))
+    stream = torch.cuda.Stream()
+    with capi.CVBatch(nf, scheme=0, form=form, stream=stream.cuda_stream) as b:
+        slots = [b.admit(int(N[k]), int(T[k]), 101 + k, k) for k in range(nf)]
+        b.set_observations(slots, obs)
+        b.run(slots)
+        b.synchronize()
+        dev_ms = []
+        for _ in range(reps):
+            b.initialize(slots)
+            b.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.run(slots)
+            e1.record(stream)
+            b.synchronize()
+            dev_ms.append(e0.elapsed_time(e1))
+        l0 = b.launches()
+        b.initialize(slots)
+        b.synchronize()
+        t0 = time.perf_counter()
+        b.set_observations(slots, obs)
+        b.run(slots)
+        lz = b.read_last(slots)["log_evidence"]
+        e2e_s = time.perf_counter() - t0
+        launches = b.launches() - l0
+    ms = statistics.median(dev_ms)
+    return {"filters_per_s": nf / (ms / 1e3), "particle_steps_per_s": psteps / (ms / 1e3),
+            "ms_per_run": ms, "e2e_filters_per_s": nf / e2e_s,
+            "h2d_bytes": int(16 * np.sum(T)), "d2h_bytes": 40 * nf,
+            "gpu_launches_per_run": launches, "log_evidence_first": float(lz[0])}
+
+
+def serving_point(capi, form, lam, seed, T=100, period_s=1e-3, max_requests=2000,
+                  budget=16 << 30):
+    """Poisson request arrivals at rate `lam`; request N log-uniform on
+    [2^10, 2^18]; each streams T observations one at a time, one every
+    `period_s` (a 1 kHz sensor).  Latency of an observation = result
+    available on the host - its arrival.  Arrivals span min(1 s,
+    max_requests / lam)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    window = min(1.0, max_requests / lam)
+    n = max(1, min(max_requests, int(rng.poisson(lam * window))))
+    arr = np.sort(rng.uniform(0.0, window, n))
+    Ns = np.exp(rng.uniform(np.log(2 ** 10), np.log(2 ** 18), n)).astype(np.int64)
+    obs = [capi.cv_simulate(T, obs_seed=5000 + k, stream_id=k) for k in range(n)]
+    ox = np.stack([o[0] for o in obs])
+    oy = np.stack([o[1] for o in obs])
+    # observation k of request r arrives at arr[r] + k * period
+    t_obs = (arr[:, None] + period_s * np.arange(T)[None, :]).ravel()
+    order = np.argsort(t_obs, kind="stable")
+    ev_r = (order // T).astype(np.int64)
+    ev_k = (order % T).astype(np.int64)
+    ev_t = t_obs[order]
+    ids = np.zeros(n, np.uint64)
+    opened = np.zeros(n, bool)
+    got = []
+    n_res = 0
+    total = n * T
+    with capi.CVServer(4096, scheme=0, form=form, hbm_budget=budget) as srv:
+        t0 = srv.now_ns()
+        i = 0
+        while n_res < total:
+            now = (srv.now_ns() - t0) * 1e-9
+            j = int(np.searchsorted(ev_t, now, side="right"))
+            if j > i:
+                rs, ks = ev_r[i:j], ev_k[i:j]
+                for r in np.unique(rs[~opened[rs]]):
+                    ids[r] = srv.open(int(Ns[r]), T, 101 + int(r), int(r))
+                    opened[r] = True
+                srv.observe(ids[rs], ox[rs, ks], oy[rs, ks],
+                            t0 + (ev_t[i:j] * 1e9).astype(np.int64))
+                for r in rs[ks == T - 1]:
+                    srv.close(int(ids[r]))
+                i = j
+            r = srv.poll(wait_ms=0 if i < total else 5)
+            if r.size:
+                got.append(r)
+                n_res += r.size
+            elif i < total:
+                time.sleep(max(0.0, min(2e-4, ev_t[i] - now)))
+        st = srv.stats()
+    res = np.concatenate(got)
+    lat = (res["done_ns"] - res["submit_ns"]) * 1e-6
+    span = (res["done_ns"].max() - res["submit_ns"].min()) * 1e-9
+    return {"rate_per_s": lam, "requests": n, "observations": int(total),
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "obs_per_s": total / span, "particle_steps_per_s": float(np.sum(Ns) * T / span),
+            "ticks": int(st["ticks"]), "max_active": int(st["max_active"]),
+            "errors": int(np.sum(res["status"] != 0))}
+
+
 def run_reference_arm(args):
     rank, world, _ = rank_env()
     if rank != 0:
@@ -186,6 +356,9 @@ def main():
     ap.add_argument("--form", default="fp64", choices=("fp64", "mixed"))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=6)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the form comparison, batched and serving sections")
+    ap.add_argument("--serving-rates", default="100,1000,10000,100000")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -294,6 +467,27 @@ def main():
     f.close()
     e2e = world * N * K / e2e_s
 
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        if args.form == "fp64":
+            extras["forms"] = forms_compare(capi, N, sch, K, W, ox, oy, sp, ms / K)
+        bN, bT, bobs = batched_workload(capi)
+        extras["batched"] = {
+            "workload": "4096 CV Student-t filters, N log-uniform [2^10, 2^16], T uniform "
+                        "[50, 500], Multinomial, threshold 0.5, seeds 101+k, streams k",
+            "filters": len(bN), "particle_steps": int(np.sum(bN * bT)),
+            "fp64": batched_run(capi, capi.FP64, bN, bT, bobs),
+            "mixed": batched_run(capi, capi.MIXED, bN, bT, bobs)}
+        b64, b32 = extras["batched"]["fp64"], extras["batched"]["mixed"]
+        extras["batched"]["speedup_mixed_vs_fp64"] = b32["filters_per_s"] / b64["filters_per_s"]
+        rates = [float(r) for r in args.serving_rates.split(",") if r]
+        extras["serving"] = {
+            "workload": "Poisson request arrivals; N log-uniform [2^10, 2^18]; T=100 "
+                        "observations per request streamed one every 1 ms; Multinomial; "
+                        "HBM budget 16 GiB; latency = result on host - arrival",
+            "fp64": [serving_point(capi, capi.FP64, lam, 11) for lam in rates],
+            "mixed": [serving_point(capi, capi.MIXED, lam, 11) for lam in rates]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -335,6 +529,7 @@ def main():
             "clocks": clk,
             "log_evidence": {"device_run": logz, "e2e_run": e2e_logz},
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -336,12 +336,13 @@ int vsmc_cuda_cv_batch_run(vsmc_cuda_cv_batch *b, uint32_t n,
                            const uint32_t *slots);
 
 /* The last step of each listed slot: ESS, log-evidence increment,
- * resampled flag and running log-evidence (host arrays of n; each may be
- * NULL).  Synchronises; returns a device error of any listed slot. */
+ * resampled flag, running log-evidence and the slot's sticky device status
+ * (host arrays of n; each may be NULL).  Synchronises; returns the first
+ * non-zero status of the listed slots (the arrays are filled either way). */
 int vsmc_cuda_cv_batch_read_last(vsmc_cuda_cv_batch *b, uint32_t n,
                                  const uint32_t *slots, double *ess,
                                  double *logz_inc, int32_t *resampled,
-                                 double *log_evidence);
+                                 double *log_evidence, int32_t *status);
 
 int vsmc_cuda_cv_batch_iter_size(vsmc_cuda_cv_batch *b, uint32_t slot,
                                  uint64_t *iter_size);
@@ -354,8 +355,83 @@ int vsmc_cuda_cv_batch_history(vsmc_cuda_cv_batch *b, uint32_t slot,
 
 int vsmc_cuda_cv_batch_synchronize(vsmc_cuda_cv_batch *b);
 
+/* vsmc_cuda_cv_batch_run records its steps in a CUDA graph and launches
+ * the graph (on by default); a run with the same slots and step counts as
+ * the previous one relaunches the same graph. */
+int vsmc_cuda_cv_batch_set_graphs(vsmc_cuda_cv_batch *b, int enable);
+
 /* Kernel launches this batch has issued. */
 int vsmc_cuda_cv_batch_launches(vsmc_cuda_cv_batch *b, uint64_t *launches);
+
+/* ---- serving: a persistent request loop over a batch ---------------------
+ *
+ * No counterpart in the reference.  A server owns a vsmc_cuda_cv_batch and
+ * one loop thread on its own stream.  Clients (any thread) open filter
+ * requests of any N and stream observations to them; each tick the loop
+ * releases finished requests, admits waiting ones in arrival order while a
+ * slot and the HBM budget allow, steps every admitted request that has a
+ * pending observation in one batched step, and publishes one result per
+ * observation.  A request's results equal those of the same filter run
+ * alone. */
+typedef struct vsmc_cuda_cv_server vsmc_cuda_cv_server;
+
+typedef struct {
+    uint64_t request;     /* id from vsmc_cuda_cv_server_open */
+    uint64_t t;           /* step (observation index) */
+    double ess;
+    double logz_inc;      /* log-evidence increment of this step */
+    double log_evidence;  /* running sum after this step */
+    int32_t resampled;
+    int32_t status;       /* VSMC_CUDA_OK or the request's error */
+    int64_t submit_ns;    /* server clock: arrival of the observation */
+    int64_t done_ns;      /* server clock: result available on the host */
+} vsmc_cuda_cv_result;
+
+typedef struct {
+    uint64_t opened, admitted, completed; /* requests */
+    uint64_t ticks, steps, particle_steps;
+    uint64_t max_active;                  /* most filters on the device */
+    uint64_t waiting, active;             /* now */
+    double busy_seconds;                  /* loop time spent in ticks */
+} vsmc_cuda_cv_server_counters;
+
+/* Starts the loop thread on the current device.  model: shared scheme,
+ * form, threshold and parameters; max_filters: slots; hbm_budget: bytes
+ * the admitted filters may hold (0 = no limit). */
+int vsmc_cuda_cv_server_create(const vsmc_cuda_cv_config *model,
+                               uint32_t max_filters, uint64_t hbm_budget,
+                               vsmc_cuda_cv_server **out);
+
+/* Stops the loop (pending work is dropped) and frees everything. */
+int vsmc_cuda_cv_server_destroy(vsmc_cuda_cv_server *s);
+
+/* The server clock (steady, nanoseconds since creation). */
+int64_t vsmc_cuda_cv_server_now_ns(vsmc_cuda_cv_server *s);
+
+/* A new filter request; VSMC_CUDA_ENOMEM if it alone exceeds the budget. */
+int vsmc_cuda_cv_server_open(vsmc_cuda_cv_server *s, uint64_t N,
+                             uint64_t T_max, uint32_t seed,
+                             uint32_t stream_id, uint64_t *request);
+
+/* The next observation of each of n requests; submit_ns (may be NULL =
+ * now) stamps their arrival on the server clock. */
+int vsmc_cuda_cv_server_observe(vsmc_cuda_cv_server *s, uint32_t n,
+                                const uint64_t *requests, const double *x,
+                                const double *y, const int64_t *submit_ns);
+
+/* No more observations: the slot is freed after the pending ones run. */
+int vsmc_cuda_cv_server_close(vsmc_cuda_cv_server *s, uint64_t request);
+
+/* Up to max results in completion order; waits up to wait_ms for one. */
+int vsmc_cuda_cv_server_poll(vsmc_cuda_cv_server *s,
+                             vsmc_cuda_cv_result *out, uint32_t max,
+                             uint32_t *n, int wait_ms);
+
+/* Waits until every submitted observation has a result. */
+int vsmc_cuda_cv_server_drain(vsmc_cuda_cv_server *s, int timeout_ms);
+
+int vsmc_cuda_cv_server_stats(vsmc_cuda_cv_server *s,
+                              vsmc_cuda_cv_server_counters *stats);
 
 #ifdef __cplusplus
 }

@@ -186,3 +186,23 @@ def test_batch_nan_observation_is_degenerate(capi):
         with pytest.raises(capi.VsmcCudaError) as e:
             b.read_last([good, bad])
         assert e.value.status == capi.EDEGENERATE
+
+
+def test_batch_graph_and_direct_runs_agree(golden, capi):
+    """A run recorded as a CUDA graph (and relaunched) equals direct launches."""
+    obs = [series(capi, golden, k, T, sid) for k, (N, T, seed, sid) in enumerate(SPECS)]
+    out = []
+    for graphs in (True, False):
+        with capi.CVBatch(len(SPECS), scheme=1, form=1) as b:
+            b.set_graphs(graphs)
+            slots = [b.admit(N, T, seed, sid) for (N, T, seed, sid) in SPECS]
+            b.set_observations(slots, obs)
+            runs = []
+            for _ in range(3):  # the second and third runs relaunch the graph
+                b.initialize(slots)
+                b.run(slots)
+                runs.append([b.history(s) for s in slots])
+            out.append(runs)
+    for r in range(3):
+        for k in range(len(SPECS)):
+            assert_same(out[0][r][k], out[1][r][k], (r, k))

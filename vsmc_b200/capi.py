@@ -42,6 +42,19 @@ class ThreefryState(C.Structure):
                 ("offset", C.c_uint64)]
 
 
+class CVResult(C.Structure):
+    _fields_ = [("request", C.c_uint64), ("t", C.c_uint64), ("ess", C.c_double),
+                ("logz_inc", C.c_double), ("log_evidence", C.c_double),
+                ("resampled", C.c_int32), ("status", C.c_int32),
+                ("submit_ns", C.c_int64), ("done_ns", C.c_int64)]
+
+
+class ServerCounters(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("opened", "admitted", "completed", "ticks", "steps",
+                                          "particle_steps", "max_active", "waiting",
+                                          "active")] + [("busy_seconds", C.c_double)]
+
+
 _lib = None
 
 
@@ -106,11 +119,22 @@ def lib():
     L.vsmc_cuda_cv_batch_initialize.argtypes = [vp, u32, vp]
     L.vsmc_cuda_cv_batch_step.argtypes = [vp, u32, vp]
     L.vsmc_cuda_cv_batch_run.argtypes = [vp, u32, vp]
-    L.vsmc_cuda_cv_batch_read_last.argtypes = [vp, u32, vp, vp, vp, vp, vp]
+    L.vsmc_cuda_cv_batch_read_last.argtypes = [vp, u32, vp, vp, vp, vp, vp, vp]
     L.vsmc_cuda_cv_batch_iter_size.argtypes = [vp, u32, C.POINTER(u64)]
     L.vsmc_cuda_cv_batch_history.argtypes = [vp, u32, vp, vp, vp, vp, vp]
     L.vsmc_cuda_cv_batch_synchronize.argtypes = [vp]
     L.vsmc_cuda_cv_batch_launches.argtypes = [vp, C.POINTER(u64)]
+    L.vsmc_cuda_cv_batch_set_graphs.argtypes = [vp, i32]
+    L.vsmc_cuda_cv_server_create.argtypes = [C.POINTER(CVConfig), u32, u64, C.POINTER(vp)]
+    L.vsmc_cuda_cv_server_destroy.argtypes = [vp]
+    L.vsmc_cuda_cv_server_now_ns.argtypes = [vp]
+    L.vsmc_cuda_cv_server_now_ns.restype = C.c_int64
+    L.vsmc_cuda_cv_server_open.argtypes = [vp, u64, u64, u32, u32, C.POINTER(u64)]
+    L.vsmc_cuda_cv_server_observe.argtypes = [vp, u32, vp, vp, vp, vp]
+    L.vsmc_cuda_cv_server_close.argtypes = [vp, u64]
+    L.vsmc_cuda_cv_server_poll.argtypes = [vp, vp, u32, C.POINTER(u32), i32]
+    L.vsmc_cuda_cv_server_drain.argtypes = [vp, i32]
+    L.vsmc_cuda_cv_server_stats.argtypes = [vp, C.POINTER(ServerCounters)]
     _lib = L
     return L
 
@@ -459,11 +483,11 @@ class CVBatch:
         import numpy as np
         a, n = self._slots(slots)
         r = dict(ess=np.zeros(n), logz_inc=np.zeros(n), resampled=np.zeros(n, np.int32),
-                 log_evidence=np.zeros(n))
+                 log_evidence=np.zeros(n), status=np.zeros(n, np.int32))
         check(lib().vsmc_cuda_cv_batch_read_last(self.h, n, a.ctypes.data,
                                                  *[_np_ptr(r[k]) for k in
                                                    ("ess", "logz_inc", "resampled",
-                                                    "log_evidence")]),
+                                                    "log_evidence", "status")]),
               "vsmc_cuda_cv_batch_read_last")
         return r
 
@@ -488,8 +512,90 @@ class CVBatch:
     def synchronize(self):
         check(lib().vsmc_cuda_cv_batch_synchronize(self.h), "vsmc_cuda_cv_batch_synchronize")
 
+    def set_graphs(self, enable=True):
+        check(lib().vsmc_cuda_cv_batch_set_graphs(self.h, 1 if enable else 0),
+              "vsmc_cuda_cv_batch_set_graphs")
+
     def launches(self) -> int:
         v = C.c_uint64()
         check(lib().vsmc_cuda_cv_batch_launches(self.h, C.byref(v)),
               "vsmc_cuda_cv_batch_launches")
         return int(v.value)
+
+
+RESULT_DTYPE = [("request", "<u8"), ("t", "<u8"), ("ess", "<f8"), ("logz_inc", "<f8"),
+                ("log_evidence", "<f8"), ("resampled", "<i4"), ("status", "<i4"),
+                ("submit_ns", "<i8"), ("done_ns", "<i8")]
+
+
+class CVServer:
+    """Persistent request loop (vsmc_cuda_cv_server): open filter requests,
+    stream observations, poll one result per observation."""
+
+    def __init__(self, max_filters, scheme=Multinomial, form=FP64, threshold=0.5,
+                 hbm_budget=0, **params):
+        import numpy as np
+        self.model = cv_config(N=2, T_max=1, scheme=scheme, form=form,
+                               threshold=threshold, **params)
+        h = C.c_void_p()
+        check(lib().vsmc_cuda_cv_server_create(C.byref(self.model), max_filters, hbm_budget,
+                                               C.byref(h)), "vsmc_cuda_cv_server_create")
+        self.h = h
+        self._buf = np.zeros(65536, dtype=RESULT_DTYPE)
+        assert self._buf.itemsize == C.sizeof(CVResult)
+
+    def close_server(self):
+        if getattr(self, "h", None):
+            check(lib().vsmc_cuda_cv_server_destroy(self.h), "vsmc_cuda_cv_server_destroy")
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close_server()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close_server()
+
+    def now_ns(self) -> int:
+        return int(lib().vsmc_cuda_cv_server_now_ns(self.h))
+
+    def open(self, N, T_max, seed=101, stream_id=0) -> int:
+        r = C.c_uint64()
+        check(lib().vsmc_cuda_cv_server_open(self.h, N, T_max, seed, stream_id, C.byref(r)),
+              "vsmc_cuda_cv_server_open")
+        return int(r.value)
+
+    def observe(self, requests, x, y, submit_ns=None):
+        import numpy as np
+        r = np.ascontiguousarray(np.atleast_1d(requests), np.uint64)
+        xa = np.ascontiguousarray(np.atleast_1d(x), np.float64)
+        ya = np.ascontiguousarray(np.atleast_1d(y), np.float64)
+        sn = None if submit_ns is None else np.ascontiguousarray(np.atleast_1d(submit_ns),
+                                                                  np.int64)
+        check(lib().vsmc_cuda_cv_server_observe(self.h, r.size, r.ctypes.data, xa.ctypes.data,
+                                                ya.ctypes.data, _np_ptr(sn)),
+              "vsmc_cuda_cv_server_observe")
+
+    def close(self, request):
+        check(lib().vsmc_cuda_cv_server_close(self.h, request), "vsmc_cuda_cv_server_close")
+
+    def poll(self, wait_ms=0):
+        """Results available now (a numpy structured array)."""
+        import numpy as np
+        n = C.c_uint32()
+        check(lib().vsmc_cuda_cv_server_poll(self.h, self._buf.ctypes.data, self._buf.size,
+                                             C.byref(n), wait_ms), "vsmc_cuda_cv_server_poll")
+        return self._buf[:n.value].copy()
+
+    def drain(self, timeout_ms=60000):
+        check(lib().vsmc_cuda_cv_server_drain(self.h, timeout_ms), "vsmc_cuda_cv_server_drain")
+
+    def stats(self) -> dict:
+        c = ServerCounters()
+        check(lib().vsmc_cuda_cv_server_stats(self.h, C.byref(c)), "vsmc_cuda_cv_server_stats")
+        return {k: getattr(c, k) for k, _ in ServerCounters._fields_}

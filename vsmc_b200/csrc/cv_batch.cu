@@ -441,6 +441,13 @@ struct vsmc_cuda_cv_batch {
     double *d_out;
     double *h_out;
     uint64_t launches;
+    // graph of the last run (vsmc_cuda_cv_batch_run)
+    bool use_graphs;
+    cudaStream_t cap_stream; // capture only; graphs launch on `stream`
+    cudaGraphExec_t run_exec;
+    std::vector<uint64_t> run_key;
+    const TileRef *run_map;
+    uint64_t run_launches;
 };
 
 namespace {
@@ -578,9 +585,9 @@ int stage_work(vsmc_cuda_cv_batch *b, const std::vector<uint32_t> &w,
 // One step of the first n work items (whose tiles are the first `tiles`
 // map entries).
 template <typename Real>
-void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles)
+void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
+                       cudaStream_t s)
 {
-    cudaStream_t s = b->stream;
     const int scheme = b->model.scheme;
     const bool residual = is_residual(scheme), sys = is_sys(scheme),
                strat = is_strat(scheme);
@@ -625,12 +632,31 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles)
     b->launches += launches;
 }
 
-void launch_step_any(vsmc_cuda_cv_batch *b, int n, long long tiles)
+void launch_step_any(vsmc_cuda_cv_batch *b, int n, long long tiles,
+                     cudaStream_t s)
 {
     if (b->model.form == VSMC_CUDA_MIXED)
-        launch_batch_step<float>(b, n, tiles);
+        launch_batch_step<float>(b, n, tiles, s);
     else
-        launch_batch_step<double>(b, n, tiles);
+        launch_batch_step<double>(b, n, tiles, s);
+}
+
+void drop_run_graph(vsmc_cuda_cv_batch *b)
+{
+    if (b->run_exec != nullptr) {
+        cudaStreamSynchronize(b->stream); // the last launch has finished
+        cudaGraphExecDestroy(b->run_exec);
+    }
+    b->run_exec = nullptr;
+    b->run_key.clear();
+}
+
+// The steps of a run: step k runs the first active(k) work items.
+void launch_run_steps(vsmc_cuda_cv_batch *b, const std::vector<int> &active,
+                      const std::vector<long long> &tile0, cudaStream_t s)
+{
+    for (int a : active)
+        launch_step_any(b, a, tile0[a], s);
 }
 
 int check_slots(const vsmc_cuda_cv_batch *b, uint32_t n,
@@ -724,6 +750,10 @@ int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
     b->d_obs = nullptr;
     b->obs_cap = 0;
     b->launches = 0;
+    b->use_graphs = true;
+    b->run_exec = nullptr;
+    b->run_map = nullptr;
+    b->run_launches = 0;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     cudaMemPoolProps props;
@@ -760,6 +790,8 @@ int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
         e = cudaMallocHost(&b->h_slot, sizeof(BatchSlot));
     if (e == cudaSuccess)
         e = cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         cudaGetLastError();
         set_last_error("vsmc_cuda_cv_batch_create: allocation failed");
@@ -802,6 +834,9 @@ int vsmc_cuda_cv_batch_destroy(vsmc_cuda_cv_batch *b)
     cudaFreeHost(b->h_out);
     cudaFreeHost(b->h_slot);
     cudaEventDestroy(b->staged);
+    drop_run_graph(b);
+    if (b->cap_stream != nullptr)
+        cudaStreamDestroy(b->cap_stream);
     cudaMemPoolDestroy(b->pool);
     cudaError_t e = cudaGetLastError();
     delete b;
@@ -1063,7 +1098,7 @@ int vsmc_cuda_cv_batch_step(vsmc_cuda_cv_batch *b, uint32_t n,
     st = stage_work(b, w, &tiles);
     if (st != VSMC_CUDA_OK)
         return st;
-    launch_step_any(b, (int)n, tiles);
+    launch_step_any(b, (int)n, tiles, b->stream);
     for (uint32_t k = 0; k < n; ++k)
         ++b->t[slots[k]];
     cudaError_t e = cudaGetLastError();
@@ -1092,18 +1127,59 @@ int vsmc_cuda_cv_batch_run(vsmc_cuda_cv_batch *b, uint32_t n,
     std::vector<long long> tile0(n + 1, 0);
     for (uint32_t k = 0; k < n; ++k)
         tile0[k + 1] = tile0[k] + b->slots[w[k]].ntiles;
-    int active = (int)n;
+    std::vector<int> active;
+    int a = (int)n;
     for (uint64_t step = 0;; ++step) {
-        while (active > 0 &&
-               b->T_obs[w[active - 1]] - b->t[w[active - 1]] <= step)
-            --active;
-        if (active == 0)
+        while (a > 0 && b->T_obs[w[a - 1]] - b->t[w[a - 1]] <= step)
+            --a;
+        if (a == 0)
             break;
-        launch_step_any(b, active, tile0[active]);
+        active.push_back(a);
+    }
+    cudaError_t e = cudaSuccess;
+    if (b->use_graphs && !active.empty()) {
+        // the whole run as one CUDA graph, reused while the work list and
+        // its step counts repeat (kernels read everything else from the
+        // slot records)
+        std::vector<uint64_t> key;
+        key.reserve(2 * n);
+        for (uint32_t k = 0; k < n; ++k) {
+            key.push_back(w[k]);
+            key.push_back(b->T_obs[w[k]] - b->t[w[k]]);
+        }
+        if (b->run_exec == nullptr || key != b->run_key ||
+            b->run_map != b->d_map) {
+            drop_run_graph(b);
+            cudaGraph_t g = nullptr;
+            e = cudaStreamBeginCapture(b->cap_stream,
+                                       cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                const uint64_t before = b->launches;
+                launch_run_steps(b, active, tile0, b->cap_stream);
+                b->run_launches = b->launches - before;
+                e = cudaStreamEndCapture(b->cap_stream, &g);
+            }
+            if (e == cudaSuccess)
+                e = cudaGraphInstantiate(&b->run_exec, g, 0);
+            if (g != nullptr)
+                cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                b->run_exec = nullptr;
+                return cuda_status(e, "vsmc_cuda_cv_batch_run: graph");
+            }
+            b->run_key = key;
+            b->run_map = b->d_map;
+            b->launches -= b->run_launches; // counted when launched
+        }
+        e = cudaGraphLaunch(b->run_exec, b->stream);
+        b->launches += b->run_launches;
+    } else {
+        launch_run_steps(b, active, tile0, b->stream);
     }
     for (uint32_t k = 0; k < n; ++k)
         b->t[slots[k]] = b->T_obs[slots[k]];
-    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaGetLastError();
     return e == cudaSuccess ? VSMC_CUDA_OK
                             : cuda_status(e, "vsmc_cuda_cv_batch_run");
 }
@@ -1111,7 +1187,7 @@ int vsmc_cuda_cv_batch_run(vsmc_cuda_cv_batch *b, uint32_t n,
 int vsmc_cuda_cv_batch_read_last(vsmc_cuda_cv_batch *b, uint32_t n,
                                  const uint32_t *slots, double *ess,
                                  double *logz_inc, int32_t *resampled,
-                                 double *log_evidence)
+                                 double *log_evidence, int32_t *status)
 {
     int st = check_slots(b, n, slots, "vsmc_cuda_cv_batch_read_last");
     if (st != VSMC_CUDA_OK)
@@ -1143,6 +1219,8 @@ int vsmc_cuda_cv_batch_read_last(vsmc_cuda_cv_batch *b, uint32_t n,
             resampled[k] = (int32_t)o[2];
         if (log_evidence)
             log_evidence[k] = o[3];
+        if (status)
+            status[k] = (int32_t)o[4];
         if (o[4] != 0.0 && err == VSMC_CUDA_OK)
             err = (int)o[4];
     }
@@ -1213,6 +1291,18 @@ int vsmc_cuda_cv_batch_synchronize(vsmc_cuda_cv_batch *b)
     cudaError_t e = cudaStreamSynchronize(b->stream);
     return e == cudaSuccess ? VSMC_CUDA_OK
                             : cuda_status(e, "vsmc_cuda_cv_batch_synchronize");
+}
+
+int vsmc_cuda_cv_batch_set_graphs(vsmc_cuda_cv_batch *b, int enable)
+{
+    if (b == nullptr)
+        return VSMC_CUDA_EINVAL;
+    b->use_graphs = enable != 0;
+    if (!b->use_graphs) {
+        cudaStreamSynchronize(b->stream);
+        drop_run_graph(b);
+    }
+    return VSMC_CUDA_OK;
 }
 
 int vsmc_cuda_cv_batch_launches(vsmc_cuda_cv_batch *b, uint64_t *launches)
