@@ -54,6 +54,24 @@ const char *vsmc_cuda_status_string(int status);
 const char *vsmc_cuda_last_error(void);
 int vsmc_cuda_abi_version(void);
 
+/* ------------------------------------------------------ device memory --- */
+
+/* Plain device memory for callers built without the CUDA toolkit (the C++
+ * interface in include/vsmc_b200/vsmc_cuda.hpp): cudaMalloc, cudaFree, and a
+ * cudaMemcpyAsync on `stream` that returns once the copy is done.  No
+ * counterpart in the reference (host memory only). */
+enum {
+    VSMC_CUDA_HOST_TO_DEVICE = 1,
+    VSMC_CUDA_DEVICE_TO_HOST = 2,
+    VSMC_CUDA_DEVICE_TO_DEVICE = 3
+};
+
+int vsmc_cuda_device_alloc(size_t bytes, void **ptr);
+int vsmc_cuda_device_free(void *ptr);
+int vsmc_cuda_memcpy(void *dst, const void *src, size_t bytes, int kind,
+                     void *stream);
+int vsmc_cuda_stream_synchronize(void *stream);
+
 /* ------------------------------------------------------------- RNG ------ */
 
 /* n successive outputs of PhiloxEngine<uint32_t,4,10>::operator()() after

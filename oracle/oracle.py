@@ -340,5 +340,26 @@ def ref_cv_filter(N, T, scheme, obs_x, obs_y, seed=101, stream=0, threshold=0.5,
     return r
 
 
+def ref_cv_summary(N, T, scheme, obs_x, obs_y, seed=101, stream=0, threshold=0.5,
+                   param=CV_DEFAULT) -> str:
+    """The summary table vSMC's `os << sampler` writes for the same filter
+    (Sampler::print, core/sampler.hpp:684-721; monitor "pos" named pos.x and
+    pos.y as in example/pf/include/pf_smp_do.hpp)."""
+    ox = np.ascontiguousarray(obs_x, np.float64)
+    oy = np.ascontiguousarray(obs_y, np.float64)
+    p = np.asarray(param, np.float64)
+    L = ref()
+    L.ref_cv_summary.restype = C.c_uint64
+    L.ref_cv_summary.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_int, C.c_double,
+                                 C.c_uint, C.c_uint, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_uint64]
+    args = (p.ctypes.data, N, T, scheme, threshold, seed, stream,
+            ox.ctypes.data, oy.ctypes.data)
+    n = L.ref_cv_summary(*args, None, 0)
+    buf = C.create_string_buffer(int(n) + 1)
+    L.ref_cv_summary(*args, buf, int(n) + 1)
+    return buf.value.decode()
+
+
 def ref_max_threads() -> int:
     return ref().ref_max_threads()

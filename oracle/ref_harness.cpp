@@ -29,6 +29,7 @@
 #include <cstdint>
 #include <cstring>
 #include <sstream>
+#include <string>
 #include <vector>
 
 namespace {
@@ -212,6 +213,7 @@ struct run_out {
     uint64_t *words_used;
     double *seconds;
     double *step_seconds;
+    std::string *summary; // Sampler::print output (sampler.hpp:684-721)
 };
 
 template <template <typename> class StateB,
@@ -274,6 +276,14 @@ double run_filter (const cv_param &prm, std::size_t N, std::size_t T,
         if (out->words_used) {
             *out->words_used =
                 threefry_words_used(sampler.particle().resample_rng());
+        }
+        if (out->summary) {
+            // monitor names as the pf example sets them (pf_smp_do.hpp)
+            sampler.monitor("pos").name(0) = "pos.x";
+            sampler.monitor("pos").name(1) = "pos.y";
+            std::stringstream ss;
+            ss << sampler;
+            *out->summary = ss.str();
         }
     }
     return sampler.particle().value().zconst;
@@ -396,7 +406,7 @@ double ref_cv_filter (int backend, int nthreads, const double *param,
     cv_param prm = {param[0], param[1], param[2], param[3], param[4],
         param[5], param[6]};
     run_out out = {ess, resampled, logz_inc, mean_x, mean_y, final_state,
-        final_lw, words_used, seconds, step_seconds};
+        final_lw, words_used, seconds, step_seconds, VSMC_NULLPTR};
     if (nthreads > 0)
         omp_set_num_threads(nthreads);
     switch (backend) {
@@ -413,6 +423,30 @@ double ref_cv_filter (int backend, int nthreads, const double *param,
                    vsmc::MoveSEQ, vsmc::MonitorEvalSEQ>(prm, N, T, scheme,
                            threshold, seed, stream, ox, oy, &out);
     }
+}
+
+// The summary table `os << sampler` writes (Sampler::print, sampler.hpp:
+// 684-721) for the CV filter on the SEQ backend, copied into `buf` (at most
+// cap bytes, NUL-terminated).  Returns the full length.
+uint64_t ref_cv_summary (const double *param, uint64_t N, uint64_t T,
+        int scheme, double threshold, unsigned seed, unsigned stream,
+        const double *ox, const double *oy, char *buf, uint64_t cap)
+{
+    cv_param prm = {param[0], param[1], param[2], param[3], param[4],
+        param[5], param[6]};
+    std::string text;
+    run_out out = {VSMC_NULLPTR, VSMC_NULLPTR, VSMC_NULLPTR, VSMC_NULLPTR,
+        VSMC_NULLPTR, VSMC_NULLPTR, VSMC_NULLPTR, VSMC_NULLPTR, VSMC_NULLPTR,
+        VSMC_NULLPTR, &text};
+    run_filter<vsmc::StateSEQ, vsmc::InitializeSEQ, vsmc::MoveSEQ,
+        vsmc::MonitorEvalSEQ>(prm, N, T, scheme, threshold, seed, stream, ox,
+                oy, &out);
+    if (buf && cap > 0) {
+        const uint64_t n = text.size() < cap - 1 ? text.size() : cap - 1;
+        std::memcpy(buf, text.data(), n);
+        buf[n] = '\0';
+    }
+    return text.size();
 }
 
 int ref_max_threads (void) {return omp_get_max_threads();}

@@ -4,6 +4,9 @@ Run from the repository root where the vSMC include tree is available:
 
     make -C oracle && python tests/golden/make_golden.py
 
+(`python tests/golden/make_golden.py summaries` rewrites only the summary
+tables cv_summary_s*.tsv.)
+
 Every array in golden.npz is produced by oracle/_ref/libvsmc_ref.so
 (oracle/ref_harness.cpp over vSMC's own Sampler, WeightSet, Resample<...>,
 internal::cfrp_trans, Philox4x32 and Threefry4x64).  The C restatement in
@@ -122,5 +125,19 @@ def main():
     print("wrote", OUT, os.path.getsize(OUT), "bytes,", len(g), "arrays")
 
 
+def write_summaries():
+    """cv_summary_s<scheme>.tsv: vSMC's `os << sampler` table for the N=1000,
+    T=100 filter of golden.npz (same observations, seed 101)."""
+    T = 100
+    ox, oy = O.cv_simulate(T, obs_seed=7)
+    here = os.path.dirname(os.path.abspath(__file__))
+    for sch in range(6):
+        text = O.ref_cv_summary(1000, T, sch, ox, oy, seed=101)
+        with open(os.path.join(here, f"cv_summary_s{sch}.tsv"), "w") as f:
+            f.write(text)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] != ["summaries"]:
+        main()
+    write_summaries()

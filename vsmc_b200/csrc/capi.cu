@@ -354,4 +354,71 @@ int vsmc_cuda_copy_f64(uint64_t N, uint32_t dim, const double *src,
                             : cuda_status(e, "vsmc_cuda_copy_f64");
 }
 
+int vsmc_cuda_device_alloc(size_t bytes, void **ptr)
+{
+    if (ptr == nullptr) {
+        set_last_error("vsmc_cuda_device_alloc: null pointer");
+        return VSMC_CUDA_EINVAL;
+    }
+    *ptr = nullptr;
+    if (bytes == 0)
+        return VSMC_CUDA_OK;
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *ptr = nullptr;
+        set_last_error("vsmc_cuda_device_alloc: cudaMalloc of " +
+                       std::to_string(bytes) + " bytes failed");
+        return VSMC_CUDA_ENOMEM;
+    }
+    return VSMC_CUDA_OK;
+}
+
+int vsmc_cuda_device_free(void *ptr)
+{
+    if (ptr == nullptr)
+        return VSMC_CUDA_OK;
+    cudaError_t e = cudaFree(ptr);
+    return e == cudaSuccess ? VSMC_CUDA_OK
+                            : cuda_status(e, "vsmc_cuda_device_free");
+}
+
+int vsmc_cuda_memcpy(void *dst, const void *src, size_t bytes, int kind,
+                     void *stream)
+{
+    cudaMemcpyKind k;
+    switch (kind) {
+    case VSMC_CUDA_HOST_TO_DEVICE:
+        k = cudaMemcpyHostToDevice;
+        break;
+    case VSMC_CUDA_DEVICE_TO_HOST:
+        k = cudaMemcpyDeviceToHost;
+        break;
+    case VSMC_CUDA_DEVICE_TO_DEVICE:
+        k = cudaMemcpyDeviceToDevice;
+        break;
+    default:
+        set_last_error("vsmc_cuda_memcpy: unknown direction");
+        return VSMC_CUDA_EINVAL;
+    }
+    if (bytes == 0)
+        return VSMC_CUDA_OK;
+    if (dst == nullptr || src == nullptr) {
+        set_last_error("vsmc_cuda_memcpy: null pointer");
+        return VSMC_CUDA_EINVAL;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, k, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? VSMC_CUDA_OK : cuda_status(e, "vsmc_cuda_memcpy");
+}
+
+int vsmc_cuda_stream_synchronize(void *stream)
+{
+    cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? VSMC_CUDA_OK
+                            : cuda_status(e, "vsmc_cuda_stream_synchronize");
+}
+
 } // extern "C"
