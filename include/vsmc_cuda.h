@@ -451,6 +451,86 @@ int vsmc_cuda_cv_server_drain(vsmc_cuda_cv_server *s, int timeout_ms);
 int vsmc_cuda_cv_server_stats(vsmc_cuda_cv_server *s,
                               vsmc_cuda_cv_server_counters *stats);
 
+/* ---- tempered SMC for a 1-D Gaussian mixture ----------------------------
+ *
+ * The sampler of example/gmm (gmm_smc.cpp) with the alpha_prior schedule
+ * (example/include/move_alpha.hpp:120-140): Seed::set(seed);
+ * Sampler<gmm_state>(N, scheme, threshold); init gmm_init (4 components);
+ * move move_smc (alpha_t = (t / iters)^power, incremental weight
+ * loglik * (alpha_t - alpha_{t-1}), example/include/move_smc.hpp:51-75);
+ * `sweeps` sweeps of gmm_move_mu, gmm_move_lambda and gmm_move_weight
+ * (example/gmm/include/gmm_move.hpp:35-117) with every block's proposal sd
+ * `sd`; path_sampling(smc_path).  Each particle draws from its own
+ * Threefry4x64 engine (RngSet<Threefry4x64, Vector>: engine i seeded with
+ * the (i+1)-th Seed::get(), the resample engine with the (N+1)-th). */
+typedef struct vsmc_cuda_gmm vsmc_cuda_gmm;
+
+typedef struct {
+    uint64_t N;       /* particles */
+    uint64_t iters;   /* tempering steps after initialize */
+    int power;        /* alpha_t = (t / iters)^power */
+    int sweeps;       /* MH sweeps per step (<= 16) */
+    double sd;        /* proposal sd of every block */
+    int scheme;       /* vsmc_cuda_scheme */
+    double threshold; /* resample when ESS < threshold * N */
+    uint32_t seed;    /* Seed::set(seed) */
+    int form;         /* VSMC_CUDA_FP64, or VSMC_CUDA_MIXED: each data
+                         point's mixture density in float, the per-particle
+                         sum of log terms in double */
+    int group;        /* lanes per particle (1, 2, 4, 8, 16); 0 = pick the
+                         fastest at initialize (results do not depend on it) */
+} vsmc_cuda_gmm_config;
+
+/* N 2^16, iters 100, power 4, sweeps 5, sd 0.1, Systematic, threshold 0.5,
+ * seed 101, FP64, group 0. */
+void vsmc_cuda_gmm_config_default(vsmc_cuda_gmm_config *cfg);
+
+/* data: n host doubles (n <= 16384), gmm_state::read_data. */
+int vsmc_cuda_gmm_create(const vsmc_cuda_gmm_config *cfg, const double *data,
+                         uint64_t n, void *stream, vsmc_cuda_gmm **out);
+int vsmc_cuda_gmm_destroy(vsmc_cuda_gmm *g);
+
+/* Sampler::initialize / iterate(num) (at most iters steps in total). */
+int vsmc_cuda_gmm_initialize(vsmc_cuda_gmm *g);
+int vsmc_cuda_gmm_iterate(vsmc_cuda_gmm *g, uint64_t num);
+int vsmc_cuda_gmm_iter_size(vsmc_cuda_gmm *g, uint64_t *iter_size);
+
+/* Histories (host arrays of iter_size entries, each may be NULL): ESS,
+ * resampled flags, log-evidence increments log sum_i W_i exp(inc_i), path
+ * sampling integrand sum_i W_i loglik_i and grid alpha_t, and acceptance
+ * counts (iter_size x (1 + 3 sweeps): move_smc's 0, then the MH moves in
+ * queue order), as Sampler::accept_history.  Synchronises. */
+int vsmc_cuda_gmm_history(vsmc_cuda_gmm *g, double *ess, int32_t *resampled,
+                          double *zinc, double *integrand, double *grid,
+                          int64_t *accept);
+
+/* log-evidence estimates with the -n/2 log(2 pi) constant: the SMC product
+ * of increments (zconst + log_likelihood_const, example/include/smc_do.hpp)
+ * and path sampling.  Synchronises. */
+int vsmc_cuda_gmm_log_evidence(vsmc_cuda_gmm *g, double *smc, double *path);
+
+/* Particles (host, N x 14: mu[4], lambda[4], weight[4], log prior, log
+ * likelihood), max-normalised log-weights and the words each particle's
+ * engine has drawn (each may be NULL).  Synchronises. */
+int vsmc_cuda_gmm_read_params(vsmc_cuda_gmm *g, double *params, double *lw,
+                              uint64_t *words);
+
+/* Log likelihood of every current particle evaluated in `form` (host, N
+ * doubles), for precision comparisons.  Synchronises. */
+int vsmc_cuda_gmm_loglik(vsmc_cuda_gmm *g, int form, double *out);
+
+/* Lanes per particle in use (the autotuned value when group was 0). */
+int vsmc_cuda_gmm_group(vsmc_cuda_gmm *g, int *group);
+
+/* CUDA-event timing of the MCMC kernels (as vsmc_cuda_cv_set_timing). */
+int vsmc_cuda_gmm_set_timing(vsmc_cuda_gmm *g, int enable);
+int vsmc_cuda_gmm_timing(vsmc_cuda_gmm *g, double *mcmc_ms, uint64_t *steps,
+                         uint64_t *launches);
+
+/* The workload's mixture data: point i from component floor(4 u) of means
+ * (-3, 0, 2, 5), unit sd; Philox4x32-10 keyed {seed, 3}. Host only. */
+int vsmc_cuda_gmm_simulate(uint32_t seed, uint64_t n, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -363,3 +363,104 @@ def ref_cv_summary(N, T, scheme, obs_x, obs_y, seed=101, stream=0, threshold=0.5
 
 def ref_max_threads() -> int:
     return ref().ref_max_threads()
+
+
+# ----------------------------------------------------------------- GMM ----
+
+GMM_REF_SO = os.path.join(HERE, "_ref", "libvsmc_gmm_ref.so")
+_gmm_ref = None
+
+
+def gmm_ref_available() -> bool:
+    return os.path.exists(GMM_REF_SO)
+
+
+def gmm_simulate(n=1000, seed=1):
+    """The mixture data (orc_gmm_simulate)."""
+    out = np.zeros(n)
+    L = lib()
+    L.orc_gmm_simulate.argtypes = [C.c_uint32, C.c_size_t, C.c_void_p]
+    L.orc_gmm_simulate.restype = None
+    L.orc_gmm_simulate(seed, n, out.ctypes.data)
+    return out
+
+
+def _gmm_outputs(N, iters, sweeps):
+    T = iters + 1
+    r = CVResult(ess=np.zeros(T), resampled=np.zeros(T, np.int32), zinc=np.zeros(T),
+                 integrand=np.zeros(T), grid=np.zeros(T),
+                 accept=np.zeros((T, 1 + 3 * sweeps), np.int64),
+                 params=np.zeros((N, 14)), lw=np.zeros(N), words=np.zeros(N, np.uint64))
+    order = ("ess", "resampled", "zinc", "integrand", "grid", "accept", "params", "lw", "words")
+    return r, [r[k].ctypes.data for k in order]
+
+
+def gmm_smc(data, N, iters=100, power=4, sweeps=5, sd=0.1, scheme=3, threshold=0.5,
+            seed=101):
+    """The tempered SMC sampler, C restatement (orc_gmm_smc)."""
+    data = np.ascontiguousarray(data, np.float64)
+    L = lib()
+    L.orc_gmm_smc.argtypes = ([C.c_void_p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_int,
+                               C.c_int, C.c_double, C.c_int, C.c_double, C.c_uint32]
+                              + [C.c_void_p] * 10)
+    L.orc_gmm_smc.restype = C.c_double
+    r, ptrs = _gmm_outputs(N, iters, sweeps)
+    pl = np.zeros(1)
+    r["logz"] = L.orc_gmm_smc(data.ctypes.data, data.size, N, iters, power, sweeps, sd,
+                              scheme, threshold, seed, *ptrs, pl.ctypes.data)
+    r["path_logz"] = float(pl[0])
+    return r
+
+
+def gmm_loglik(data, mu, lam, weight):
+    L = lib()
+    L.orc_gmm_loglik.argtypes = [C.c_void_p, C.c_size_t] + [C.c_void_p] * 3
+    L.orc_gmm_loglik.restype = C.c_double
+    data = np.ascontiguousarray(data, np.float64)
+    a = [np.ascontiguousarray(v, np.float64) for v in (mu, lam, weight)]
+    return L.orc_gmm_loglik(data.ctypes.data, data.size, *[v.ctypes.data for v in a])
+
+
+def gmm_ref():
+    global _gmm_ref
+    if _gmm_ref is None:
+        if not os.path.exists(GMM_REF_SO):
+            build()
+        if not os.path.exists(GMM_REF_SO):
+            raise RuntimeError("GMM reference harness not built (vSMC tree absent)")
+        L = C.CDLL(GMM_REF_SO)
+        L.ref_gmm_smc.argtypes = ([C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_int,
+                                   C.c_int, C.c_double, C.c_int, C.c_double, C.c_uint,
+                                   C.c_int] + [C.c_void_p] * 11)
+        L.ref_gmm_smc.restype = C.c_double
+        L.ref_gmm_summary.argtypes = ([C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_int,
+                                       C.c_double, C.c_int, C.c_double, C.c_uint, C.c_void_p,
+                                       C.c_uint64])
+        L.ref_gmm_summary.restype = C.c_uint64
+        _gmm_ref = L
+    return _gmm_ref
+
+
+def ref_gmm_smc(data, N, iters=100, power=4, sweeps=5, sd=0.1, scheme=3, threshold=0.5,
+                seed=101, nthreads=0):
+    """The same sampler through vSMC with the reference's example/gmm classes."""
+    data = np.ascontiguousarray(data, np.float64)
+    r, ptrs = _gmm_outputs(N, iters, sweeps)
+    pl, sec = np.zeros(1), np.zeros(1)
+    r["logz"] = gmm_ref().ref_gmm_smc(data.ctypes.data, data.size, N, iters, power, sweeps,
+                                      sd, scheme, threshold, seed, nthreads, *ptrs,
+                                      pl.ctypes.data, sec.ctypes.data)
+    r["path_logz"] = float(pl[0])
+    r["seconds"] = float(sec[0])
+    return r
+
+
+def ref_gmm_summary(data, N, iters=100, sweeps=5, sd=0.1, scheme=3, threshold=0.5,
+                    seed=101) -> str:
+    data = np.ascontiguousarray(data, np.float64)
+    L = gmm_ref()
+    args = (data.ctypes.data, data.size, N, iters, sweeps, sd, scheme, threshold, seed)
+    n = L.ref_gmm_summary(*args, None, 0)
+    buf = C.create_string_buffer(int(n) + 1)
+    L.ref_gmm_summary(*args, buf, int(n) + 1)
+    return buf.value.decode()

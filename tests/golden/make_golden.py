@@ -5,7 +5,8 @@ Run from the repository root where the vSMC include tree is available:
     make -C oracle && python tests/golden/make_golden.py
 
 (`python tests/golden/make_golden.py summaries` rewrites only the summary
-tables cv_summary_s*.tsv.)
+tables cv_summary_s*.tsv; `... gmm` only gmm.npz and gmm_summary.tsv, the
+tempered SMC sampler of oracle/ref_gmm.cpp.)
 
 Every array in golden.npz is produced by oracle/_ref/libvsmc_ref.so
 (oracle/ref_harness.cpp over vSMC's own Sampler, WeightSet, Resample<...>,
@@ -137,7 +138,38 @@ def write_summaries():
             f.write(text)
 
 
+GMM_OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "gmm.npz")
+# the tempered SMC fixture: N, iters, power, sweeps, sd, scheme, threshold, seed
+GMM_RUN = dict(N=512, iters=20, power=4, sweeps=5, sd=0.1, scheme=3, threshold=0.5,
+               seed=101)
+
+
+def write_gmm():
+    """gmm.npz: the tempered SMC sampler of example/gmm through vSMC
+    (oracle/ref_gmm.cpp) on 1000 mixture points (seed 1)."""
+    data = O.gmm_simulate(1000, 1)
+    r = O.ref_gmm_smc(data, **GMM_RUN)
+    g = {"data": data}
+    for k in ("ess", "resampled", "zinc", "integrand", "grid", "accept", "params", "lw",
+              "words"):
+        g[k] = r[k]
+    g["logz"] = np.array(r["logz"])
+    g["path_logz"] = np.array(r["path_logz"])
+    for k, v in GMM_RUN.items():
+        g["run_" + k] = np.array(v)
+    np.savez_compressed(GMM_OUT, **g)
+    text = O.ref_gmm_summary(data, GMM_RUN["N"], GMM_RUN["iters"], GMM_RUN["sweeps"],
+                             GMM_RUN["sd"], GMM_RUN["scheme"], GMM_RUN["threshold"],
+                             GMM_RUN["seed"])
+    with open(os.path.join(os.path.dirname(GMM_OUT), "gmm_summary.tsv"), "w") as f:
+        f.write(text)
+
+
 if __name__ == "__main__":
-    if sys.argv[1:] != ["summaries"]:
-        main()
-    write_summaries()
+    if sys.argv[1:] == ["gmm"]:
+        write_gmm()
+    else:
+        if sys.argv[1:] != ["summaries"]:
+            main()
+            write_gmm()
+        write_summaries()

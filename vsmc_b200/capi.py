@@ -55,6 +55,13 @@ class ServerCounters(C.Structure):
                                           "active")] + [("busy_seconds", C.c_double)]
 
 
+class GmmConfig(C.Structure):
+    _fields_ = [("N", C.c_uint64), ("iters", C.c_uint64), ("power", C.c_int),
+                ("sweeps", C.c_int), ("sd", C.c_double), ("scheme", C.c_int),
+                ("threshold", C.c_double), ("seed", C.c_uint32), ("form", C.c_int),
+                ("group", C.c_int)]
+
+
 _lib = None
 
 
@@ -135,6 +142,21 @@ def lib():
     L.vsmc_cuda_cv_server_poll.argtypes = [vp, vp, u32, C.POINTER(u32), i32]
     L.vsmc_cuda_cv_server_drain.argtypes = [vp, i32]
     L.vsmc_cuda_cv_server_stats.argtypes = [vp, C.POINTER(ServerCounters)]
+    L.vsmc_cuda_gmm_config_default.argtypes = [C.POINTER(GmmConfig)]
+    L.vsmc_cuda_gmm_config_default.restype = None
+    L.vsmc_cuda_gmm_create.argtypes = [C.POINTER(GmmConfig), vp, u64, vp, C.POINTER(vp)]
+    L.vsmc_cuda_gmm_destroy.argtypes = [vp]
+    L.vsmc_cuda_gmm_initialize.argtypes = [vp]
+    L.vsmc_cuda_gmm_iterate.argtypes = [vp, u64]
+    L.vsmc_cuda_gmm_iter_size.argtypes = [vp, C.POINTER(u64)]
+    L.vsmc_cuda_gmm_history.argtypes = [vp] + [vp] * 6
+    L.vsmc_cuda_gmm_log_evidence.argtypes = [vp, C.POINTER(f64), C.POINTER(f64)]
+    L.vsmc_cuda_gmm_read_params.argtypes = [vp, vp, vp, vp]
+    L.vsmc_cuda_gmm_loglik.argtypes = [vp, i32, vp]
+    L.vsmc_cuda_gmm_group.argtypes = [vp, C.POINTER(C.c_int)]
+    L.vsmc_cuda_gmm_set_timing.argtypes = [vp, i32]
+    L.vsmc_cuda_gmm_timing.argtypes = [vp, C.POINTER(f64), C.POINTER(u64), C.POINTER(u64)]
+    L.vsmc_cuda_gmm_simulate.argtypes = [u32, u64, vp]
     _lib = L
     return L
 
@@ -599,3 +621,112 @@ class CVServer:
         c = ServerCounters()
         check(lib().vsmc_cuda_cv_server_stats(self.h, C.byref(c)), "vsmc_cuda_cv_server_stats")
         return {k: getattr(c, k) for k, _ in ServerCounters._fields_}
+
+
+# ------------------------------------------------------------- GMM -------
+
+def gmm_simulate(n=1000, seed=1):
+    """The mixture data (host computation, no device)."""
+    import numpy as np
+    out = np.zeros(n)
+    check(lib().vsmc_cuda_gmm_simulate(seed, n, out.ctypes.data), "vsmc_cuda_gmm_simulate")
+    return out
+
+
+class GmmSampler:
+    """Tempered SMC sampler for the 1-D Gaussian mixture (vsmc_cuda_gmm):
+    ``initialize()`` and ``iterate(n)`` as vsmc::Sampler."""
+
+    def __init__(self, data, N=1 << 16, iters=100, power=4, sweeps=5, sd=0.1,
+                 scheme=Systematic, threshold=0.5, seed=101, form=FP64, group=0, stream=None):
+        import numpy as np
+        c = GmmConfig()
+        lib().vsmc_cuda_gmm_config_default(C.byref(c))
+        for k, v in dict(N=N, iters=iters, power=power, sweeps=sweeps, sd=sd, scheme=scheme,
+                         threshold=threshold, seed=seed, form=form, group=group).items():
+            setattr(c, k, v)
+        self.cfg = c
+        self.N, self.sweeps = N, sweeps
+        d = np.ascontiguousarray(data, np.float64)
+        h = C.c_void_p()
+        check(lib().vsmc_cuda_gmm_create(C.byref(c), d.ctypes.data, d.size, stream, C.byref(h)),
+              "vsmc_cuda_gmm_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            check(lib().vsmc_cuda_gmm_destroy(self.h), "vsmc_cuda_gmm_destroy")
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def initialize(self):
+        check(lib().vsmc_cuda_gmm_initialize(self.h), "vsmc_cuda_gmm_initialize")
+
+    def iterate(self, num=1):
+        check(lib().vsmc_cuda_gmm_iterate(self.h, num), "vsmc_cuda_gmm_iterate")
+
+    def iter_size(self) -> int:
+        v = C.c_uint64()
+        check(lib().vsmc_cuda_gmm_iter_size(self.h, C.byref(v)), "vsmc_cuda_gmm_iter_size")
+        return int(v.value)
+
+    def history(self):
+        import numpy as np
+        T = self.iter_size()
+        r = dict(ess=np.zeros(T), resampled=np.zeros(T, np.int32), zinc=np.zeros(T),
+                 integrand=np.zeros(T), grid=np.zeros(T),
+                 accept=np.zeros((T, 1 + 3 * self.sweeps), np.int64))
+        check(lib().vsmc_cuda_gmm_history(self.h, *[_np_ptr(r[k]) for k in
+                                                    ("ess", "resampled", "zinc", "integrand",
+                                                     "grid", "accept")]),
+              "vsmc_cuda_gmm_history")
+        return r
+
+    def log_evidence(self):
+        """(SMC estimate, path-sampling estimate)."""
+        a, b = C.c_double(), C.c_double()
+        check(lib().vsmc_cuda_gmm_log_evidence(self.h, C.byref(a), C.byref(b)),
+              "vsmc_cuda_gmm_log_evidence")
+        return a.value, b.value
+
+    def read_params(self):
+        import numpy as np
+        p = np.zeros((self.N, 14))
+        lw = np.zeros(self.N)
+        w = np.zeros(self.N, np.uint64)
+        check(lib().vsmc_cuda_gmm_read_params(self.h, p.ctypes.data, lw.ctypes.data,
+                                              w.ctypes.data), "vsmc_cuda_gmm_read_params")
+        return p, lw, w
+
+    def loglik(self, form):
+        import numpy as np
+        out = np.zeros(self.N)
+        check(lib().vsmc_cuda_gmm_loglik(self.h, form, out.ctypes.data), "vsmc_cuda_gmm_loglik")
+        return out
+
+    def group(self) -> int:
+        v = C.c_int()
+        check(lib().vsmc_cuda_gmm_group(self.h, C.byref(v)), "vsmc_cuda_gmm_group")
+        return v.value
+
+    def set_timing(self, enable=True):
+        check(lib().vsmc_cuda_gmm_set_timing(self.h, 1 if enable else 0),
+              "vsmc_cuda_gmm_set_timing")
+
+    def timing(self):
+        """(mcmc_ms, steps, launches)."""
+        a, b, c = C.c_double(), C.c_uint64(), C.c_uint64()
+        check(lib().vsmc_cuda_gmm_timing(self.h, C.byref(a), C.byref(b), C.byref(c)),
+              "vsmc_cuda_gmm_timing")
+        return a.value, int(b.value), int(c.value)

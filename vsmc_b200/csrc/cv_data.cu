@@ -1,5 +1,5 @@
-// cv_data.cu -- host-side simulation of the CV Student-t observation series
-// (the workload's synthetic data): state (0, 0, 1, 1), constant-velocity
+// cv_data.cu -- host-side simulation of the workloads' synthetic data.  The
+// CV Student-t observation series: state (0, 0, 1, 1), constant-velocity
 // moves with Gaussian noise, positions observed with Student-t(nu) noise of
 // scale 1/scale.  Step t uses a Philox4x32-10 engine keyed {obs_seed, 1}
 // with counter {0, t, 0, stream_id} and one std::normal_distribution, so the
@@ -53,6 +53,28 @@ extern "C" int vsmc_cuda_cv_simulate(const vsmc_cuda_cv_config *c,
         if (truth != nullptr)
             for (int d = 0; d != 4; ++d)
                 truth[t * 4 + d] = s[d];
+    }
+    return VSMC_CUDA_OK;
+}
+
+// The mixture data of the tempered SMC workload: point i draws its
+// component k = floor(4 u) (u from std::uniform_real_distribution) and then
+// mean_k + std::normal_distribution(0, 1) noise, means (-3, 0, 2, 5), on one
+// Philox4x32-10 engine keyed {seed, 3} with counter 0.
+extern "C" int vsmc_cuda_gmm_simulate(uint32_t seed, uint64_t n, double *out)
+{
+    if (out == nullptr)
+        return VSMC_CUDA_EINVAL;
+    static const double means[4] = {-3.0, 0.0, 2.0, 5.0};
+    vsmc_b200::Philox4x32 eng(vsmc_b200::Philox4x32::key_type{{seed, 3u}});
+    std::uniform_real_distribution<double> u01(0, 1);
+    typedef std::normal_distribution<double> normal;
+    normal nd;
+    for (uint64_t i = 0; i != n; ++i) {
+        const double u = u01(eng);
+        int k = static_cast<int>(u * 4.0);
+        k = k > 3 ? 3 : k;
+        out[i] = nd(eng, normal::param_type(means[k], 1.0));
     }
     return VSMC_CUDA_OK;
 }
