@@ -319,6 +319,68 @@ def serving_point(capi, form, lam, seed, T=100, period_s=1e-3, max_requests=2000
             "errors": int(np.sum(res["status"] != 0))}
 
 
+# Nominal FP32 CUDA-core peak of a B200 (148 SMs x 128 lanes x 2 flops x
+# 1965 MHz) and its special-function (exp2 / log2) rate (16 per SM per
+# clock); MEASURED_PEAKS.json holds no FP32 figure.
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+SFU_PEAK_TOPS = 148 * 16 * 1.965e9 / 1e12
+GMM_FLOPS_PER_POINT = 21  # 4 components x (sub, mul, mul, exp, fma) + log
+
+
+def gmm_run(capi, form, data, N=1 << 16, iters=100, sweeps=5, seed=101):
+    """The tempered SMC sampler (N = 2^16, 100 steps of alpha_t =
+    (t/100)^4, 5 sweeps of the three MH block moves, sd 0.1, Systematic at
+    ESS < N/2): device time of initialize + all steps, the MCMC kernels'
+    share, and their FP32 flop / special-function rates."""
+    import torch
+
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    with capi.GmmSampler(data, N=N, iters=iters, sweeps=sweeps, form=form, seed=seed,
+                         stream=sp) as s:
+        s.initialize()  # picks the lanes per particle
+        G = s.group()
+    with capi.GmmSampler(data, N=N, iters=iters, sweeps=sweeps, form=form, seed=seed,
+                         group=G, stream=sp) as s:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s.set_timing(True)
+        e0.record(stream)
+        s.initialize()
+        s.iterate(iters)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        mcmc_ms, steps, launches = s.timing()
+        logz, path = s.log_evidence()
+        h = s.history()
+    points = float(N) * iters * 3 * sweeps * len(data)
+    flops = points * GMM_FLOPS_PER_POINT
+    return {"ms_per_run": ms, "mcmc_ms": mcmc_ms, "lanes_per_particle": G,
+            "particle_steps_per_s": N * iters / (ms / 1e3),
+            "mcmc_gflops": flops / (mcmc_ms / 1e3) / 1e9,
+            "mcmc_fp32_frac_of_nominal": flops / (mcmc_ms / 1e3) / 1e12 / FP32_PEAK_TFLOPS,
+            "mcmc_sfu_frac_of_nominal": 5 * points / (mcmc_ms / 1e3) / 1e12 / SFU_PEAK_TOPS,
+            "log_evidence": logz, "path_log_evidence": path,
+            "resampled_steps": int(h["resampled"].sum()), "gpu_launches": launches}
+
+
+def gmm_cpu_reference(data, N=2048, iters=100, sweeps=5):
+    """vSMC's own example/gmm sampler (oracle/_ref, OpenMP, all threads) on
+    the same schedule with fewer particles (the per-particle work does not
+    depend on N): particle-steps/s."""
+    from oracle import oracle as O
+
+    if not O.gmm_ref_available():
+        return None
+    r = O.ref_gmm_smc(data, N, iters=iters, sweeps=sweeps)
+    return {"value": N * iters / r["seconds"], "unit": "particle-steps/s",
+            "cores": O.ref_max_threads(), "kind": "reference",
+            "sample": f"vSMC example/gmm sampler, StateOMP, N={N}, {iters} steps, "
+                      f"{sweeps} sweeps ({r['seconds']:.1f} s)"}
+
+
 def run_reference_arm(args):
     rank, world, _ = rank_env()
     if rank != 0:
@@ -480,6 +542,19 @@ def main():
             "mixed": batched_run(capi, capi.MIXED, bN, bT, bobs)}
         b64, b32 = extras["batched"]["fp64"], extras["batched"]["mixed"]
         extras["batched"]["speedup_mixed_vs_fp64"] = b32["filters_per_s"] / b64["filters_per_s"]
+        gdata = capi.gmm_simulate(1000, 1)
+        g64 = gmm_run(capi, capi.FP64, gdata)
+        g32 = gmm_run(capi, capi.MIXED, gdata)
+        extras["gmm"] = {
+            "workload": "tempered SMC, 1-D Gaussian mixture: 1000 points from means "
+                        "(-3, 0, 2, 5), N=2^16, 100 steps alpha_t=(t/100)^4, 5 RWMH sweeps "
+                        "(mu, log-precision, logit blocks; sd 0.1), Systematic at ESS < N/2",
+            "fp64": g64, "mixed": g32,
+            "speedup_mixed_vs_fp64": g64["ms_per_run"] / g32["ms_per_run"],
+            "roofline": {"bound": "fp32 special-function units (4 exp2 + 1 log2 per point)",
+                         "peak_fp32_tflops_nominal": FP32_PEAK_TFLOPS,
+                         "peak_sfu_tops_nominal": SFU_PEAK_TOPS},
+            "cpu_baseline": gmm_cpu_reference(gdata) if not args.no_cpu_baseline else None}
         rates = [float(r) for r in args.serving_rates.split(",") if r]
         extras["serving"] = {
             "workload": "Poisson request arrivals; N log-uniform [2^10, 2^18]; T=100 "
