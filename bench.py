@@ -421,11 +421,23 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the form comparison, batched and serving sections")
     ap.add_argument("--serving-rates", default="100,1000,10000,100000")
+    ap.add_argument("--gmm-only", choices=("fp64", "mixed"),
+                    help="run only the tempered SMC sampler in this form (profiling)")
+    ap.add_argument("--gmm-iters", type=int, default=100)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.gmm_only:
+        from vsmc_b200 import capi
+
+        capi.lib()
+        form = capi.MIXED if args.gmm_only == "mixed" else capi.FP64
+        r = gmm_run(capi, form, capi.gmm_simulate(1000, 1), iters=args.gmm_iters)
+        print(json.dumps({"workload": f"tempered SMC N=2^16 {args.gmm_iters} steps "
+                                      f"{args.gmm_only}", **r}), flush=True)
+        return 0
 
     import numpy as np
     import torch

@@ -29,8 +29,8 @@
 // Forms: FP64 evaluates the likelihood in double throughout (the reference
 // arithmetic, one rounding per operation in the reference's order); MIXED
 // evaluates each data point's mixture density in float (exp2 / log2 on the
-// special-function units) and accumulates the per-point log terms of a
-// particle in double.  Everything else is double in both.
+// special-function units, one log2 per pair of points) and accumulates the
+// log terms of a particle in double.  Everything else is double in both.
 #include "cv_kernels.cuh"
 
 #include <cmath>
@@ -75,6 +75,13 @@ struct GmmState {
     double mu[kGmmK], lam[kGmmK], loglam[kGmmK], w[kGmmK];
     double lp, ll, lt;
 };
+
+// One out-of-line copy of the double log / exp / sqrt for the proposal and
+// acceptance code: inlined at every call site they made the kernel too large
+// for the instruction cache (warps stalled waiting for instructions).
+static __device__ __noinline__ double mh_log(double x) { return log(x); }
+static __device__ __noinline__ double mh_exp(double x) { return exp(x); }
+static __device__ __noinline__ double mh_sqrt(double x) { return sqrt(x); }
 
 // One particle's Threefry4x64 engine: key {seed_i, 0, 0, 0}; the word at
 // position `off` is lane off % 4 of block ctr = off / 4 + 1 (the counter is
@@ -144,7 +151,7 @@ struct NormalDist {
                 y = 2.0 * r.canonical() - 1.0;
                 r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
             } while (r2 > 1.0 || r2 == 0.0);
-            const double mult = sqrt(__ddiv_rn(-2.0 * log(r2), r2));
+            const double mult = mh_sqrt(__ddiv_rn(-2.0 * mh_log(r2), r2));
             saved = __dmul_rn(x, mult);
             avail = true;
             ret = __dmul_rn(y, mult);
@@ -174,8 +181,8 @@ __device__ __forceinline__ double gamma_draw(NormalDist &nd, ParticleRng &r,
             break;
         const double rhs = __dadd_rn(
             __dmul_rn(__dmul_rn(0.5, n), n),
-            __dmul_rn(a1, __dadd_rn(__dadd_rn(1.0, -v), log(v))));
-        if (!(log(u) > rhs))
+            __dmul_rn(a1, __dadd_rn(__dadd_rn(1.0, -v), mh_log(v))));
+        if (!(mh_log(u) > rhs))
             break;
     }
     if (alpha == malpha)
@@ -184,6 +191,36 @@ __device__ __forceinline__ double gamma_draw(NormalDist &nd, ParticleRng &r,
         u = r.canonical();
     while (u == 0.0);
     return pow(u, 1.0 / alpha) * a1 * v * beta;
+}
+
+// Special-function unit instructions (PTX ex2.approx.ftz.f32 and
+// lg2.approx.ftz.f32): 2^x and log2 x in float, subnormals flushed to 0.
+__device__ __forceinline__ float sfu_ex2(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float sfu_lg2(float x)
+{
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// MIXED form: the mixture density of one point plus the reference's 1e-13
+// floor, in float.
+__device__ __forceinline__ float mix_density(float x, const float *m,
+                                             const float *A, const float *B)
+{
+    float lli = 0.0f;
+#pragma unroll
+    for (int d = 0; d < kGmmK; ++d) {
+        const float r = __fsub_rn(x, m[d]);
+        lli = __fadd_rn(lli, sfu_ex2(__fmaf_rn(-B[d], __fmul_rn(r, r), A[d])));
+    }
+    return __fadd_rn(lli, 1e-13f);
 }
 
 // The likelihood's sum over the data points has one fixed order whatever
@@ -215,22 +252,19 @@ __device__ __forceinline__ double gmm_loglik(const GmmState &s,
             A[d] = (float)(log2(s.w[d]) + 0.5 * s.loglam[d] * kLog2e);
             B[d] = (float)(0.5 * s.lam[d] * kLog2e);
         }
+        // Points i and i + 16 of a class share one log: log2 of the
+        // product of their densities (each >= 1e-13, so the product stays
+        // a normal float); the class adds these pair terms in double.
         const float *x = static_cast<const float *>(data);
-        for (int base = 0; base < n; base += kLlClasses) {
+        for (int base = 0; base < n; base += 2 * kLlClasses) {
 #pragma unroll
             for (int j = 0; j < J; ++j) {
                 const int i = base + g + j * G;
                 if (i < n) {
-                    float lli = 0.0f;
-#pragma unroll
-                    for (int d = 0; d < kGmmK; ++d) {
-                        const float r = __fsub_rn(x[i], m[d]);
-                        const float q = __fmul_rn(r, r);
-                        lli = __fadd_rn(lli,
-                                        exp2f(__fmaf_rn(-B[d], q, A[d])));
-                    }
-                    acc[j] = __dadd_rn(
-                        acc[j], (double)log2f(__fadd_rn(lli, 1e-13f)));
+                    float p = mix_density(x[i], m, A, B);
+                    if (i + kLlClasses < n)
+                        p = __fmul_rn(p, mix_density(x[i + kLlClasses], m, A, B));
+                    acc[j] = __dadd_rn(acc[j], (double)sfu_lg2(p));
                 }
             }
         }
@@ -285,7 +319,7 @@ __device__ __forceinline__ double gmm_log_prior(const GmmState &s,
         const double resid = __dsub_rn(s.mu[d], a.mu0);
         lp = __dadd_rn(lp, __ddiv_rn(__dmul_rn(-0.5, __dmul_rn(resid, resid)),
                                      sd02));
-        lp = __dadd_rn(lp, __dsub_rn(__dmul_rn(a.shape0 - 1, log(s.lam[d])),
+        lp = __dadd_rn(lp, __dsub_rn(__dmul_rn(a.shape0 - 1, s.loglam[d]),
                                      __ddiv_rn(s.lam[d], a.scale0)));
     }
     return lp;
@@ -300,8 +334,8 @@ __device__ __forceinline__ void gmm_log_target(GmmState &s, const GmmArgs &a,
 {
 #pragma unroll
     for (int d = 0; d < kGmmK; ++d)
-        s.loglam[d] = log(s.lam[d]);
-    s.lp = gmm_log_prior(s, a);
+        s.loglam[d] = mh_log(s.lam[d]);
+    s.lp = gmm_log_prior(s, a); // its log(lambda_d) is loglam[d]
     s.ll = gmm_loglik<G, F32>(s, data, a.n, g, mask);
     s.lt = __dadd_rn(s.lp, __dmul_rn(a.alpha, s.ll));
 }
@@ -314,9 +348,9 @@ __device__ __forceinline__ double logit_term(const double *w)
     for (int d = 0; d < kGmmK - 1; ++d) {
         const double r = __ddiv_rn(w[d], w[kGmmK - 1]);
         sum_lw = __dadd_rn(sum_lw, r);
-        sum_llw = __dadd_rn(sum_llw, log(r));
+        sum_llw = __dadd_rn(sum_llw, mh_log(r));
     }
-    return __dsub_rn(sum_llw, __dmul_rn((double)kGmmK, log(sum_lw)));
+    return __dsub_rn(sum_llw, __dmul_rn((double)kGmmK, mh_log(sum_lw)));
 }
 
 // The three block moves (gmm_move.hpp:35-117); each returns 1 if accepted.
@@ -342,14 +376,14 @@ __device__ __forceinline__ int gmm_move_block(int block, GmmState &s,
         for (int d = 0; d < kGmmK; ++d)
             s.lam[d] = __dmul_rn(
                 s.lam[d],
-                exp(__dadd_rn(__dmul_rn(a.sd, nd(rng, 0.0, 1.0)), 0.0)));
+                mh_exp(__dadd_rn(__dmul_rn(a.sd, nd(rng, 0.0, 1.0)), 0.0)));
     } else {
         double sum_weight = 1.0;
 #pragma unroll
         for (int d = 0; d < kGmmK - 1; ++d) {
-            double v = log(__ddiv_rn(s.w[d], s.w[kGmmK - 1]));
+            double v = mh_log(__ddiv_rn(s.w[d], s.w[kGmmK - 1]));
             v = __dadd_rn(v, nd(rng, 0.0, a.sd));
-            v = exp(v);
+            v = mh_exp(v);
             s.w[d] = v;
             sum_weight = __dadd_rn(sum_weight, v);
         }
@@ -370,7 +404,7 @@ __device__ __forceinline__ int gmm_move_block(int block, GmmState &s,
     }
     const double p = block == 0 ? __dsub_rn(s.lt, lt_old)
                                 : __dadd_rn(__dsub_rn(s.lt, lt_old), extra);
-    const double u = log(rng.canonical());
+    const double u = mh_log(rng.canonical());
     if (p < u) {
         s = o;
         s.lt = lt_old;
@@ -402,7 +436,7 @@ __device__ __forceinline__ void load_state(GmmState &s, const GmmBuf &b,
         s.mu[d] = b.base[d * N + i];
         s.lam[d] = b.base[(4 + d) * N + i];
         s.w[d] = b.base[(8 + d) * N + i];
-        s.loglam[d] = log(s.lam[d]);
+        s.loglam[d] = mh_log(s.lam[d]);
     }
     s.lp = b.base[12 * N + i];
     s.ll = b.base[13 * N + i];
@@ -442,18 +476,18 @@ __device__ __forceinline__ const void *stage_data(const GmmArgs &a,
     return smem;
 }
 
-// Per-CTA acceptance counts (integer sums: any order gives the same).
-__device__ __forceinline__ void cta_reduce_acc(const long long *acc, int nacc,
+// Per-CTA acceptance counts (integer sums: any order gives the same).  Bit
+// m of `acc` is 1 if this thread's particle accepted move m.
+__device__ __forceinline__ void cta_reduce_acc(uint64_t acc, int nacc,
                                                long long *tile_acc)
 {
     __shared__ long long sh_acc[kGmmThreads / 32][kGmmMaxAcc];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int k = 0; k < nacc; ++k) {
-        long long v = acc[k];
-        for (int o = 16; o > 0; o >>= 1)
-            v += __shfl_xor_sync(0xffffffffu, v, o);
+        const unsigned votes =
+            __ballot_sync(0xffffffffu, (unsigned)((acc >> k) & 1u));
         if (lane == 0)
-            sh_acc[wid][k] = v;
+            sh_acc[wid][k] = __popc(votes);
     }
     __syncthreads();
     if (threadIdx.x < nacc) {
@@ -468,7 +502,7 @@ __device__ __forceinline__ void cta_reduce_acc(const long long *acc, int nacc,
 // alpha 0, log-weight 0.  Each engine continues from its stored position
 // (the RngSet outlives Sampler::initialize).
 template <int G, bool F32>
-__global__ void __launch_bounds__(kGmmThreads)
+__global__ void __launch_bounds__(kGmmThreads, 2)
 k_gmm_init(GmmArgs a, double *lw)
 {
     extern __shared__ __align__(16) unsigned char gmm_smem[];
@@ -505,15 +539,12 @@ k_gmm_init(GmmArgs a, double *lw)
         a.words[i] = rng.off;
         lw[i] = 0.0;
     }
-    long long acc[kGmmMaxAcc];
-    for (int k = 0; k < kGmmMaxAcc; ++k)
-        acc[k] = 0;
-    cta_reduce_acc(acc, 3 * a.sweeps, a.tile_acc);
+    cta_reduce_acc(0, 3 * a.sweeps, a.tile_acc);
 }
 
 // One MCMC stage: gather (if this step resampled), sweeps x 3 MH moves.
 template <int G, bool F32>
-__global__ void __launch_bounds__(kGmmThreads)
+__global__ void __launch_bounds__(kGmmThreads, 2)
 k_gmm_mcmc(GmmArgs a)
 {
     extern __shared__ __align__(16) unsigned char gmm_smem[];
@@ -534,24 +565,23 @@ k_gmm_mcmc(GmmArgs a)
     load_state(s, a.src, a.N, src);
     ParticleRng rng;
     rng.init(particle_key(a.seed_base, i), a.words[i]);
-    long long acc[kGmmMaxAcc];
-    const int nacc = 3 * a.sweeps;
-    for (int k = 0; k < kGmmMaxAcc; ++k)
-        acc[k] = 0;
+    uint64_t acc = 0; // bit 3k + b: sweep k's move b accepted
+#pragma unroll 1
     for (int k = 0; k < a.sweeps; ++k)
+#pragma unroll 1
         for (int b = 0; b < 3; ++b)
-            acc[3 * k + b] = gmm_move_block<G, F32>(b, s, rng, a, data, g,
-                                                    mask);
+            acc |= (uint64_t)gmm_move_block<G, F32>(b, s, rng, a, data, g,
+                                                    mask)
+                   << (3 * k + b);
     __syncwarp();
     const bool leader = active && g == 0;
     if (leader) {
         store_state(s, a.dst, a.N, i);
         a.words[i] = rng.off;
     } else {
-        for (int k = 0; k < nacc; ++k)
-            acc[k] = 0;
+        acc = 0;
     }
-    cta_reduce_acc(acc, nacc, a.tile_acc);
+    cta_reduce_acc(acc, 3 * a.sweeps, a.tile_acc);
 }
 
 // Likelihood only (autotuning and precision checks): ll of every particle
