@@ -51,6 +51,11 @@ constexpr int kGmmMaxAcc = 3 * kGmmMaxSweeps;
 constexpr int kGmmMaxData = 16384;    // data points held in shared memory
 constexpr int kGmmParamArrays = 14;   // mu[4], lambda[4], weight[4], lp, ll
 
+// CTAs per SM the MCMC and init kernels are compiled for (register cap).
+#ifndef VSMC_GMM_MIN_BLOCKS
+#define VSMC_GMM_MIN_BLOCKS 2
+#endif
+
 // SoA parameter buffer: array a of particle i at base[a * N + i].
 struct GmmBuf {
     double *base;
@@ -83,6 +88,15 @@ static __device__ __noinline__ double mh_log(double x) { return log(x); }
 static __device__ __noinline__ double mh_exp(double x) { return exp(x); }
 static __device__ __noinline__ double mh_sqrt(double x) { return sqrt(x); }
 
+// One Threefry4x64-20 block, out of line for the same reason.
+static __device__ __noinline__ u64x4 mh_threefry(uint64_t ctr0, u64x4 key)
+{
+    u64x4 c;
+    c.v[0] = ctr0;
+    c.v[1] = c.v[2] = c.v[3] = 0;
+    return threefry4x64_20(c, key);
+}
+
 // One particle's Threefry4x64 engine: key {seed_i, 0, 0, 0}; the word at
 // position `off` is lane off % 4 of block ctr = off / 4 + 1 (the counter is
 // incremented before each block, utility/counter.hpp).
@@ -104,10 +118,7 @@ struct ParticleRng {
     {
         const uint64_t b = off >> 2;
         if (b != blk) {
-            u64x4 c;
-            c.v[0] = b + 1;
-            c.v[1] = c.v[2] = c.v[3] = 0;
-            const u64x4 w = threefry4x64_20(c, key);
+            const u64x4 w = mh_threefry(b + 1, key);
             b0 = w.v[0];
             b1 = w.v[1];
             b2 = w.v[2];
@@ -502,7 +513,7 @@ __device__ __forceinline__ void cta_reduce_acc(uint64_t acc, int nacc,
 // alpha 0, log-weight 0.  Each engine continues from its stored position
 // (the RngSet outlives Sampler::initialize).
 template <int G, bool F32>
-__global__ void __launch_bounds__(kGmmThreads, 2)
+__global__ void __launch_bounds__(kGmmThreads, VSMC_GMM_MIN_BLOCKS)
 k_gmm_init(GmmArgs a, double *lw)
 {
     extern __shared__ __align__(16) unsigned char gmm_smem[];
@@ -544,7 +555,7 @@ k_gmm_init(GmmArgs a, double *lw)
 
 // One MCMC stage: gather (if this step resampled), sweeps x 3 MH moves.
 template <int G, bool F32>
-__global__ void __launch_bounds__(kGmmThreads, 2)
+__global__ void __launch_bounds__(kGmmThreads, VSMC_GMM_MIN_BLOCKS)
 k_gmm_mcmc(GmmArgs a)
 {
     extern __shared__ __align__(16) unsigned char gmm_smem[];
@@ -901,12 +912,20 @@ double alpha_at(uint64_t t, uint64_t iters, int power)
     return a;
 }
 
-// Picks the lanes per particle with the fastest likelihood kernel on the
-// current particles (CUDA events, best of 3 per candidate).  The choice
-// changes no result: the likelihood's summation order does not depend on it.
+// Picks the lanes per particle with the fastest MCMC sweep on the current
+// particles (CUDA events, best of 3 per candidate).  The trial sweeps write
+// into the spare parameter buffer and a copy of the engine positions, so
+// the sampler's state is untouched; and the choice changes no result, the
+// likelihood's summation order not depending on it.  The proposal and
+// acceptance work is repeated in every lane of a group, so the fastest G
+// balances it against the split data loop.
 int autotune_group(vsmc_cuda_gmm *g)
 {
-    GmmArgs a = gmm_args(g, g->cur, g->cur);
+    GmmArgs a = gmm_args(g, g->cur, 1 - g->cur);
+    a.words = reinterpret_cast<uint64_t *>(g->scratch);
+    a.sweeps = 1;
+    cudaMemcpyAsync(a.words, g->words, g->cfg.N * 8, cudaMemcpyDeviceToDevice,
+                    g->stream);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -914,13 +933,14 @@ int autotune_group(vsmc_cuda_gmm *g)
     int best = 4;
     float best_ms = 1e30f;
     for (int c = 0; c < 5; ++c) {
+        const unsigned grid = (unsigned)gmm_ntiles_mcmc(a.N, cand[c]);
         float ms_min = 1e30f;
         for (int r = 0; r < 3; ++r) {
             cudaEventRecord(e0, g->stream);
             if (gmm_f32(g))
-                launch_loglik_t<true>(g, a, cand[c], g->scratch);
+                launch_mcmc_t<true>(g, a, cand[c], grid);
             else
-                launch_loglik_t<false>(g, a, cand[c], g->scratch);
+                launch_mcmc_t<false>(g, a, cand[c], grid);
             cudaEventRecord(e1, g->stream);
             cudaEventSynchronize(e1);
             float ms = 0.0f;
