@@ -561,17 +561,25 @@ k_sorted_uniforms_body(EngineRef eng, const ResampleCtl *ctl,
         uv[j] = __dadd_rn(1.0, -exp(lmax));
         tmax = fmax(tmax, uv[j]);
     }
-    // block exclusive max-scan
-    shm[threadIdx.x] = tmax;
-    __syncthreads();
-    for (int o = 1; o < kThreads; o <<= 1) {
-        const double v = threadIdx.x >= (unsigned)o ? shm[threadIdx.x - o]
-                                                    : -INFINITY;
-        __syncthreads();
-        shm[threadIdx.x] = fmax(shm[threadIdx.x], v);
-        __syncthreads();
+    // block exclusive max-scan (max is exact, so any order gives the same
+    // values): inclusive warp scan, then the maxima of the earlier warps
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double inc = tmax;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o)
+            inc = fmax(inc, v);
     }
-    double m = threadIdx.x > 0 ? fmax(umax, shm[threadIdx.x - 1]) : umax;
+    if (lane == 31)
+        shm[wid] = inc;
+    double exc = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane == 0)
+        exc = -INFINITY;
+    __syncthreads();
+    for (int w = 0; w < wid; ++w)
+        exc = fmax(exc, shm[w]);
+    double m = fmax(umax, exc);
     const int kb = ctl->kbits;
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
@@ -896,8 +904,12 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     }
 }
 
+#ifndef VSMC_INVERT_MIN_BLOCKS
+#define VSMC_INVERT_MIN_BLOCKS 5
+#endif
+
 template <typename W, bool Residual, bool Sys>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, VSMC_INVERT_MIN_BLOCKS)
 k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
          const long long *tile_kexcl, const double *u, long long n_u,
          const int32_t *L, int32_t *rep_out, int32_t *copy_from,
