@@ -233,7 +233,7 @@ kb_sorted_uniforms(const BatchSlot *slots, const TileRef *map)
 }
 
 template <typename Real, bool Residual, bool Sys>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, VSMC_INVERT_MIN_BLOCKS)
 kb_invert(const BatchSlot *slots, const TileRef *map)
 {
     __shared__ SmemInvert<Residual> sm;

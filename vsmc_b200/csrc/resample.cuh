@@ -150,6 +150,14 @@ __device__ __forceinline__ double residual_split(double w, double Nd,
     return modf(__dmul_rn(Nd, w), &k);
 }
 
+// The latency-bound per-tile kernels of the sorted sequence and the cfrp
+// fill are compiled for eight CTAs per SM (32 registers): more warps in
+// flight hide their dependent loads.
+#ifndef VSMC_SCAN_MIN_BLOCKS
+#define VSMC_SCAN_MIN_BLOCKS 8
+#endif
+#define VSMC_SCAN_BOUNDS kThreads, VSMC_SCAN_MIN_BLOCKS
+
 // Shared memory of each per-tile body (the __global__ wrappers declare one;
 // a caller that runs several bodies in one CTA can overlay them).
 struct SmemTileSums {
@@ -494,7 +502,7 @@ k_sorted_tile_sums_body(EngineRef eng, const ResampleCtl *ctl, double *tile_sum,
         tile_sum[bid] = total;
 }
 
-static __global__ void __launch_bounds__(kThreads)
+static __global__ void __launch_bounds__(VSMC_SCAN_BOUNDS)
 k_sorted_tile_sums(EngineRef eng, const ResampleCtl *ctl, double *tile_sum,
                    double *u)
 {
@@ -592,7 +600,7 @@ k_sorted_uniforms_body(EngineRef eng, const ResampleCtl *ctl,
     }
 }
 
-static __global__ void __launch_bounds__(kThreads)
+static __global__ void __launch_bounds__(VSMC_SCAN_BOUNDS)
 k_sorted_uniforms(EngineRef eng, const ResampleCtl *ctl,
                   const double *tile_excl, double *u, int32_t *L)
 {
@@ -1078,7 +1086,7 @@ k_cfrp_fill_body(long long N, ResampleCtl *ctl, const int32_t *sinc_local,
     }
 }
 
-static __global__ void __launch_bounds__(kThreads)
+static __global__ void __launch_bounds__(VSMC_SCAN_BOUNDS)
 k_cfrp_fill(long long N, ResampleCtl *ctl, const int32_t *sinc_local,
             const int32_t *zexcl, const int32_t *tfirst, const int32_t *tlast,
             int32_t *copy_from)
