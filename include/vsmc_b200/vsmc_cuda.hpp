@@ -20,6 +20,8 @@
 //   vsmc::Particle<T>              -> vsmc_b200::ParticleCUDA<Dim>
 //   vsmc::Sampler<cv_state> of example/pf
 //                                  -> vsmc_b200::CVSampler (the fused filter)
+//   vsmc::Sampler<gmm_state> of example/gmm (tempered SMC)
+//                                  -> vsmc_b200::GmmSampler
 //   (no counterpart)               -> vsmc_b200::CVBatch, CVServer
 #ifndef VSMC_B200_VSMC_CUDA_HPP
 #define VSMC_B200_VSMC_CUDA_HPP
@@ -578,6 +580,162 @@ class CVSampler
 template <typename CharT, typename Traits>
 inline std::basic_ostream<CharT, Traits> &operator<<(
     std::basic_ostream<CharT, Traits> &os, const CVSampler &s)
+{
+    return s.print(os);
+}
+
+// The tempered SMC sampler of example/gmm (gmm_smc.cpp with alpha_prior,
+// move_smc, the three MH block moves and path sampling), on the device.
+// Seeded like the reference from Seed: the N particle engines take the
+// next N Seed::get() values and the resample engine the one after.
+class GmmSampler
+{
+  public:
+    typedef std::size_t size_type;
+
+    GmmSampler(const double *data, std::size_t n, size_type N,
+               std::size_t iters = 100, int power = 4, int sweeps = 5,
+               double sd = 0.1, ResampleScheme scheme = Systematic,
+               double threshold = 0.5, Form form = FP64,
+               void *stream = nullptr)
+        : g_(nullptr), N_(N), sweeps_(sweeps), iter_(0), cached_(false)
+    {
+        vsmc_cuda_gmm_config cfg;
+        vsmc_cuda_gmm_config_default(&cfg);
+        cfg.N = N;
+        cfg.iters = iters;
+        cfg.power = power;
+        cfg.sweeps = sweeps;
+        cfg.sd = sd;
+        cfg.scheme = scheme;
+        cfg.threshold = threshold;
+        cfg.form = form;
+        Seed &s = Seed::instance();
+        cfg.seed = s.seed();
+        for (size_type i = 0; i != N + 1; ++i)
+            s.get();
+        check(vsmc_cuda_gmm_create(&cfg, data, n, stream, &g_),
+              "vsmc_cuda_gmm_create");
+    }
+    GmmSampler(const GmmSampler &) = delete;
+    GmmSampler &operator=(const GmmSampler &) = delete;
+    ~GmmSampler() { vsmc_cuda_gmm_destroy(g_); }
+
+    size_type size() const { return N_; }
+    std::size_t iter_size() const { return iter_; }
+
+    GmmSampler &initialize()
+    {
+        check(vsmc_cuda_gmm_initialize(g_), "vsmc_cuda_gmm_initialize");
+        iter_ = 1;
+        cached_ = false;
+        return *this;
+    }
+
+    GmmSampler &iterate(std::size_t num = 1)
+    {
+        check(vsmc_cuda_gmm_iterate(g_, num), "vsmc_cuda_gmm_iterate");
+        iter_ += num;
+        cached_ = false;
+        return *this;
+    }
+
+    double ess_history(std::size_t iter) const { return hist().ess[iter]; }
+    bool resampled_history(std::size_t iter) const
+    {
+        return hist().resampled[iter] != 0;
+    }
+    // Sampler::accept_history(id, iter): id 0 is move_smc, then the MH
+    // moves in queue order
+    std::size_t accept_history(std::size_t id, std::size_t iter) const
+    {
+        return static_cast<std::size_t>(
+            hist().accept[iter * (1 + 3 * sweeps_) + id]);
+    }
+
+    // zconst + log_likelihood_const (example/include/smc_do.hpp)
+    double log_evidence() const
+    {
+        double smc = 0, path = 0;
+        check(vsmc_cuda_gmm_log_evidence(g_, &smc, &path),
+              "vsmc_cuda_gmm_log_evidence");
+        return smc;
+    }
+    double path_log_evidence() const
+    {
+        double smc = 0, path = 0;
+        check(vsmc_cuda_gmm_log_evidence(g_, &smc, &path),
+              "vsmc_cuda_gmm_log_evidence");
+        return path;
+    }
+
+    // Sampler::print: Size, Resampled, Accept.k, ESS, Path.Integrand,
+    // Path.Grid (core/sampler.hpp:566-721).
+    template <typename CharT, typename Traits>
+    std::basic_ostream<CharT, Traits> &print(
+        std::basic_ostream<CharT, Traits> &os, char sepchar = '\t') const
+    {
+        if (iter_ == 0 || !os.good())
+            return os;
+        const History &h = hist();
+        const std::size_t nacc = 1 + 3 * static_cast<std::size_t>(sweeps_);
+        os << "Size" << sepchar << "Resampled" << sepchar;
+        for (std::size_t k = 0; k != nacc; ++k)
+            os << "Accept." << k << sepchar;
+        os << "ESS" << sepchar << "Path.Integrand" << sepchar << "Path.Grid"
+           << sepchar << '\n';
+        for (std::size_t t = 0; t != iter_; ++t) {
+            os << N_ << sepchar << (h.resampled[t] != 0 ? 1 : 0) << sepchar;
+            for (std::size_t k = 0; k != nacc; ++k)
+                os << h.accept[t * nacc + k] << sepchar;
+            os << h.ess[t] << sepchar << h.integrand[t] << sepchar
+               << h.grid[t] << sepchar << '\n';
+        }
+        return os;
+    }
+
+    vsmc_cuda_gmm *handle() { return g_; }
+
+  private:
+    struct History {
+        std::vector<double> ess, zinc, integrand, grid;
+        std::vector<std::int32_t> resampled;
+        std::vector<std::int64_t> accept;
+    };
+
+    vsmc_cuda_gmm *g_;
+    size_type N_;
+    int sweeps_;
+    std::size_t iter_;
+    mutable bool cached_;
+    mutable History h_;
+
+    const History &hist() const
+    {
+        if (!cached_) {
+            const std::size_t T = iter_;
+            h_.ess.resize(T);
+            h_.zinc.resize(T);
+            h_.integrand.resize(T);
+            h_.grid.resize(T);
+            h_.resampled.resize(T);
+            h_.accept.resize(T * (1 + 3 * static_cast<std::size_t>(sweeps_)));
+            if (T > 0)
+                check(vsmc_cuda_gmm_history(g_, h_.ess.data(),
+                                            h_.resampled.data(),
+                                            h_.zinc.data(),
+                                            h_.integrand.data(),
+                                            h_.grid.data(), h_.accept.data()),
+                      "vsmc_cuda_gmm_history");
+            cached_ = true;
+        }
+        return h_;
+    }
+};
+
+template <typename CharT, typename Traits>
+inline std::basic_ostream<CharT, Traits> &operator<<(
+    std::basic_ostream<CharT, Traits> &os, const GmmSampler &s)
 {
     return s.print(os);
 }

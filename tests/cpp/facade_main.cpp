@@ -14,6 +14,10 @@
 //   facade_main weights N lw.bin inc.bin w.bin
 //       WeightSetCUDA: set_log_weight(lw), add_log_weight(inc), read_weight;
 //       prints the ESS.
+//   facade_main gmm N iters sweeps scheme data.bin n out.tsv
+//       Seed::set(101); GmmSampler over the n doubles of data.bin (alpha_t =
+//       (t/iters)^4, sd 0.1, threshold 0.5); writes `os << sampler` and
+//       prints the SMC and path log-evidence.
 //   facade_main particle N scheme seed out.bin
 //       ParticleCUDA<2>: state (i, -i), weights from log-weights
 //       -((i mod 7) - 3)^2, resample(scheme, 1.0); writes the resampled
@@ -173,6 +177,29 @@ int particle(int argc, char **argv)
     return 0;
 }
 
+int gmm(int argc, char **argv)
+{
+    if (argc != 9)
+        return 2;
+    const std::size_t N = std::strtoull(argv[2], nullptr, 10);
+    const std::size_t iters = std::strtoull(argv[3], nullptr, 10);
+    const int sweeps = std::atoi(argv[4]);
+    const int scheme = std::atoi(argv[5]);
+    const std::size_t n = std::strtoull(argv[7], nullptr, 10);
+    std::vector<double> data = read_bin<double>(argv[6], n);
+    vsmc_b200::Seed::instance().set(101);
+    vsmc_b200::GmmSampler sampler(
+        data.data(), n, N, iters, 4, sweeps, 0.1,
+        static_cast<vsmc_b200::ResampleScheme>(scheme), 0.5);
+    sampler.initialize();
+    sampler.iterate(iters);
+    std::ofstream est(argv[8]);
+    est << sampler;
+    std::printf("%.17g %.17g\n", sampler.log_evidence(),
+                sampler.path_log_evidence());
+    return 0;
+}
+
 } // namespace
 
 int main(int argc, char **argv)
@@ -189,6 +216,8 @@ int main(int argc, char **argv)
             return weights(argc, argv);
         if (cmd == "particle")
             return particle(argc, argv);
+        if (cmd == "gmm")
+            return gmm(argc, argv);
     } catch (const vsmc_b200::RuntimeError &e) {
         std::fprintf(stderr, "RuntimeError %d: %s\n", e.status(), e.what());
         return 3;

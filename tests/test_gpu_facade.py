@@ -119,3 +119,20 @@ def test_particle_resample(exe, tmp_path, sch):
     assert int(words) == ref_words
     x = np.fromfile(out, np.float64)
     assert np.array_equal(x, cf.astype(np.float64))
+
+
+def test_gmm_sampler_summary_matches_reference(exe, tmp_path):
+    """GmmSampler prints the same table as vSMC's `os << sampler` for the
+    tempered SMC run of tests/golden/gmm.npz (Size, Resampled, the
+    acceptance counts of move_smc and the 15 MH moves, ESS, path sampling)."""
+    g = np.load(os.path.join(GOLDEN, "gmm.npz"))
+    data = tmp_path / "data.bin"
+    g["data"].tofile(data)
+    out = tmp_path / "gmm.tsv"
+    smc, path = map(float, run(exe, "gmm", int(g["run_N"]), int(g["run_iters"]),
+                               int(g["run_sweeps"]), int(g["run_scheme"]), data,
+                               g["data"].size, out))
+    with open(os.path.join(GOLDEN, "gmm_summary.tsv")) as f:
+        assert out.read_text() == f.read()
+    assert abs(smc - float(g["logz"])) <= 1e-9 * abs(float(g["logz"]))
+    assert abs(path - float(g["path_logz"])) <= 1e-9 * abs(float(g["path_logz"]))
