@@ -215,11 +215,12 @@ def batched_workload(capi, n_filters=4096, seed=2024):
     return N, T, obs
 
 
-def batched_run(capi, form, N, T, obs, reps=3):
+def batched_run(capi, form, N, T, obs, reps=3, autotune=True):
     """Every filter run to the end of its series in one batch: the run is
     one CUDA graph (a step = one launch per kernel over all live filters'
-    tiles).  Device time with CUDA events; e2e adds the observation upload
-    from host memory and the log-evidence read back."""
+    tiles), at the launch shape the batch's autotuner picks (untimed).
+    Device time with CUDA events; e2e adds the observation upload from host
+    memory and the log-evidence read back."""
     import numpy as np
     import torch
 
@@ -229,6 +230,7 @@ def batched_run(capi, form, N, T, obs, reps=3):
     with capi.CVBatch(nf, scheme=0, form=form, stream=stream.cuda_stream) as b:
         slots = [b.admit(int(N[k]), int(T[k]), 101 + k, k) for k in range(nf)]
         b.set_observations(slots, obs)
+        shape = b.autotune(slots) if autotune else (3, 1024)
         b.run(slots)
         b.synchronize()
         dev_ms = []
@@ -255,7 +257,8 @@ def batched_run(capi, form, N, T, obs, reps=3):
     return {"filters_per_s": nf / (ms / 1e3), "particle_steps_per_s": psteps / (ms / 1e3),
             "ms_per_run": ms, "e2e_filters_per_s": nf / e2e_s,
             "h2d_bytes": int(16 * np.sum(T)), "d2h_bytes": 40 * nf,
-            "gpu_launches_per_run": launches, "log_evidence_first": float(lz[0])}
+            "gpu_launches_per_run": launches, "log_evidence_first": float(lz[0]),
+            "launch_shape": {"move_ctas_per_sm": shape[0], "finalize_threads": shape[1]}}
 
 
 def serving_point(capi, form, lam, seed, T=100, period_s=1e-3, max_requests=2000,

@@ -378,6 +378,25 @@ int vsmc_cuda_cv_batch_synchronize(vsmc_cuda_cv_batch *b);
  * the previous one relaunches the same graph. */
 int vsmc_cuda_cv_batch_set_graphs(vsmc_cuda_cv_batch *b, int enable);
 
+/* The launch shape of later steps: the move compiled for `move_blocks`
+ * (2, 3 or 4) CTAs per SM, the finalize CTA at `final_threads` (1024 or
+ * 256; 256 applies only while every admitted filter has at most 256 tiles
+ * of 2048 particles).  No shape changes a result.  New batches start at
+ * (3, 1024). */
+int vsmc_cuda_cv_batch_set_launch_shape(vsmc_cuda_cv_batch *b,
+                                        int move_blocks, int final_threads);
+
+/* The batch's autotuner: times a few steps of a trial copy of (a sample
+ * of at most 256 of) the listed filters, with zero observations, under each
+ * launch shape (the move compiled for 2, 3 or 4 CTAs per SM; the finalize
+ * CTA at 1024 or 256 threads when every filter has at most 256 tiles) and
+ * keeps the fastest for later steps.  The shapes change no result, and the
+ * trial touches none of the batch's filters.  Synchronises; reports the
+ * choice (each pointer may be NULL). */
+int vsmc_cuda_cv_batch_autotune(vsmc_cuda_cv_batch *b, uint32_t n,
+                                const uint32_t *slots, int *move_blocks,
+                                int *final_threads);
+
 /* Kernel launches this batch has issued. */
 int vsmc_cuda_cv_batch_launches(vsmc_cuda_cv_batch *b, uint64_t *launches);
 

@@ -206,3 +206,41 @@ def test_batch_graph_and_direct_runs_agree(golden, capi):
     for r in range(3):
         for k in range(len(SPECS)):
             assert_same(out[0][r][k], out[1][r][k], (r, k))
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_batch_launch_shapes_agree(golden, capi, form):
+    """Every launch shape (move CTAs per SM, finalize width) and the
+    autotuner's choice give the same results bit for bit; the narrow
+    finalize is skipped for a batch holding a filter of more than 256
+    tiles."""
+    specs = SPECS + [(1 << 20, 6, 14, 8)]
+    for big in (False, True):
+        sp = specs if big else SPECS
+        obs = [series(capi, golden, k, T, sid) for k, (N, T, seed, sid) in enumerate(sp)]
+        out = {}
+        for shape in ((3, 1024), (2, 1024), (4, 256), (3, 256), "auto"):
+            with capi.CVBatch(len(sp), scheme=5 if big else 3, form=form) as b:
+                slots = [b.admit(N, T, seed, sid) for (N, T, seed, sid) in sp]
+                b.set_observations(slots, obs)
+                if shape == "auto":
+                    mv, fin = b.autotune(slots)
+                    assert mv in (2, 3, 4) and fin in (256, 1024)
+                    if big:
+                        assert fin == 1024
+                else:
+                    b.set_launch_shape(*shape)
+                b.run(slots)
+                out[shape] = [b.history(s) for s in slots]
+                out[shape].append(b.read_last(slots)["log_evidence"])
+        for shape, h in out.items():
+            for k in range(len(sp)):
+                assert_same(h[k], out[(3, 1024)][k], (big, shape, k))
+            assert np.array_equal(h[-1], out[(3, 1024)][-1])
+
+
+def test_batch_launch_shape_rejects(capi):
+    with capi.CVBatch(2, scheme=0) as b:
+        for shape in ((1, 1024), (5, 1024), (3, 512)):
+            with pytest.raises(capi.VsmcCudaError):
+                b.set_launch_shape(*shape)

@@ -132,6 +132,9 @@ def lib():
     L.vsmc_cuda_cv_batch_synchronize.argtypes = [vp]
     L.vsmc_cuda_cv_batch_launches.argtypes = [vp, C.POINTER(u64)]
     L.vsmc_cuda_cv_batch_set_graphs.argtypes = [vp, i32]
+    L.vsmc_cuda_cv_batch_set_launch_shape.argtypes = [vp, C.c_int, C.c_int]
+    L.vsmc_cuda_cv_batch_autotune.argtypes = [vp, u32, vp, C.POINTER(C.c_int),
+                                              C.POINTER(C.c_int)]
     L.vsmc_cuda_cv_server_create.argtypes = [C.POINTER(CVConfig), u32, u64, C.POINTER(vp)]
     L.vsmc_cuda_cv_server_destroy.argtypes = [vp]
     L.vsmc_cuda_cv_server_now_ns.argtypes = [vp]
@@ -533,6 +536,19 @@ class CVBatch:
 
     def synchronize(self):
         check(lib().vsmc_cuda_cv_batch_synchronize(self.h), "vsmc_cuda_cv_batch_synchronize")
+
+    def set_launch_shape(self, move_blocks, final_threads):
+        check(lib().vsmc_cuda_cv_batch_set_launch_shape(self.h, move_blocks, final_threads),
+              "vsmc_cuda_cv_batch_set_launch_shape")
+
+    def autotune(self, slots):
+        """Pick the launch shapes by timing a trial copy; returns
+        (move CTAs per SM, finalize threads)."""
+        a, n = self._slots(slots)
+        mv, fin = C.c_int(), C.c_int()
+        check(lib().vsmc_cuda_cv_batch_autotune(self.h, n, a.ctypes.data, C.byref(mv),
+                                                C.byref(fin)), "vsmc_cuda_cv_batch_autotune")
+        return mv.value, fin.value
 
     def set_graphs(self, enable=True):
         check(lib().vsmc_cuda_cv_batch_set_graphs(self.h, 1 if enable else 0),

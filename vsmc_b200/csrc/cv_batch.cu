@@ -111,8 +111,10 @@ static __global__ void kb_expand(const BatchSlot *slots, const int32_t *work,
         map[tile0[w] + k] = TileRef{slot, k};
 }
 
-template <typename Real>
-__global__ void __launch_bounds__(kThreads, VSMC_MOVE_MIN_BLOCKS)
+// MinBlocks: CTAs per SM the move is compiled for (a tuning choice of
+// vsmc_cuda_cv_batch_autotune; every variant computes the same values).
+template <typename Real, int MinBlocks>
+__global__ void __launch_bounds__(kThreads, MinBlocks)
 kb_move(const BatchSlot *slots, const TileRef *map, CVParam p)
 {
     __shared__ double sh_w[7 * kMoveWarps];
@@ -448,6 +450,10 @@ struct vsmc_cuda_cv_batch {
     std::vector<uint64_t> run_key;
     const TileRef *run_map;
     uint64_t run_launches;
+    // launch shapes (vsmc_cuda_cv_batch_autotune); no result depends on them
+    int tune_move;        // CTAs per SM the move is compiled for: 2, 3, 4
+    int tune_final;       // finalize CTA size: 256 or 1024
+    int max_ntiles;       // largest slot admitted, in tiles
 };
 
 namespace {
@@ -595,8 +601,21 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
     const BatchSlot *sl = b->d_slots;
     const TileRef *map = b->d_map;
     const int32_t *work = b->d_work;
-    kb_move<Real><<<nt, kThreads, 0, s>>>(sl, map, b->bc.p);
-    kb_finalize<<<n, kFinalThreads, 0, s>>>(sl, work, b->bc);
+    switch (b->tune_move) {
+    case 2:
+        kb_move<Real, 2><<<nt, kThreads, 0, s>>>(sl, map, b->bc.p);
+        break;
+    case 4:
+        kb_move<Real, 4><<<nt, kThreads, 0, s>>>(sl, map, b->bc.p);
+        break;
+    default:
+        kb_move<Real, 3><<<nt, kThreads, 0, s>>>(sl, map, b->bc.p);
+        break;
+    }
+    // a finalize CTA narrower than 1024 threads gives the same sums only
+    // while every slot has at most 256 tiles
+    kb_finalize<<<n, b->max_ntiles <= 256 ? b->tune_final : kFinalThreads, 0,
+                  s>>>(sl, work, b->bc);
     int launches = 2;
     if (residual) {
         kb_tile_sums<Real, true><<<nt, kThreads, 0, s>>>(sl, map);
@@ -751,6 +770,9 @@ int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
     b->obs_cap = 0;
     b->launches = 0;
     b->use_graphs = true;
+    b->tune_move = 3;
+    b->tune_final = kFinalThreads;
+    b->max_ntiles = 0;
     b->run_exec = nullptr;
     b->run_map = nullptr;
     b->run_launches = 0;
@@ -900,6 +922,8 @@ int vsmc_cuda_cv_batch_admit(vsmc_cuda_cv_batch *b, uint64_t N,
     kb_reset_slot<<<1, 32, 0, b->stream>>>(b->d_slots, (int)s);
     ++b->launches;
     b->mem[s] = m;
+    if (r.ntiles > b->max_ntiles)
+        b->max_ntiles = r.ntiles;
     b->bytes[s] = bytes;
     b->in_use += bytes;
     b->t[s] = 0;
@@ -1302,6 +1326,112 @@ int vsmc_cuda_cv_batch_set_graphs(vsmc_cuda_cv_batch *b, int enable)
         cudaStreamSynchronize(b->stream);
         drop_run_graph(b);
     }
+    return VSMC_CUDA_OK;
+}
+
+int vsmc_cuda_cv_batch_set_launch_shape(vsmc_cuda_cv_batch *b,
+                                        int move_blocks, int final_threads)
+{
+    if (b == nullptr || move_blocks < 2 || move_blocks > 4 ||
+        (final_threads != kFinalThreads && final_threads != 256)) {
+        set_last_error("vsmc_cuda_cv_batch_set_launch_shape: invalid "
+                       "arguments");
+        return VSMC_CUDA_EINVAL;
+    }
+    if (move_blocks != b->tune_move || final_threads != b->tune_final) {
+        drop_run_graph(b); // recorded with the old shapes
+        b->tune_move = move_blocks;
+        b->tune_final = final_threads;
+    }
+    return VSMC_CUDA_OK;
+}
+
+int vsmc_cuda_cv_batch_autotune(vsmc_cuda_cv_batch *b, uint32_t n,
+                                const uint32_t *slots, int *move_blocks,
+                                int *final_threads)
+{
+    int st = check_slots(b, n, slots, "vsmc_cuda_cv_batch_autotune");
+    if (st != VSMC_CUDA_OK)
+        return st;
+    if (n == 0)
+        return VSMC_CUDA_OK;
+    // a sample of the listed filters (every k-th, at most 256 of them and
+    // 1 GiB of trial memory) in a trial batch of its own, with zero
+    // observations: the trial's steps touch none of this batch's slots
+    constexpr uint64_t kTrialT = 8;
+    constexpr uint64_t kTrialBytes = 1ull << 30;
+    const uint32_t k = (n + 255) / 256;
+    std::vector<uint32_t> pick;
+    uint64_t trial_bytes = 0;
+    for (uint32_t i = 0; i < n; i += k) {
+        const uint64_t by = slot_bytes(b->model, b->slots[slots[i]].N, kTrialT);
+        if (!pick.empty() && trial_bytes + by > kTrialBytes)
+            break;
+        pick.push_back(slots[i]);
+        trial_bytes += by;
+    }
+    const uint32_t m = (uint32_t)pick.size();
+    vsmc_cuda_cv_batch *t = nullptr;
+    st = vsmc_cuda_cv_batch_create(&b->model, m, 0, b->stream, &t);
+    if (st != VSMC_CUDA_OK)
+        return st;
+    t->use_graphs = false;
+    std::vector<uint32_t> ts(m);
+    std::vector<uint64_t> T(m, kTrialT);
+    std::vector<double> zero(m * kTrialT, 0.0);
+    for (uint32_t i = 0; i < m && st == VSMC_CUDA_OK; ++i) {
+        const BatchSlot &r = b->slots[pick[i]];
+        st = vsmc_cuda_cv_batch_admit(t, (uint64_t)r.N, kTrialT, 101 + i,
+                                      r.stream_id, &ts[i]);
+    }
+    if (st == VSMC_CUDA_OK)
+        st = vsmc_cuda_cv_batch_set_observations(t, m, ts.data(), T.data(),
+                                                 zero.data(), zero.data(), 0);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best_move = b->tune_move, best_final = b->tune_final;
+    float best_ms = 1e30f;
+    const int moves[3] = {2, 3, 4};
+    const int finals[2] = {kFinalThreads, 256};
+    const int nfinal = t->max_ntiles <= 256 ? 2 : 1;
+    for (int im = 0; im < 3 && st == VSMC_CUDA_OK; ++im)
+        for (int jf = 0; jf < nfinal && st == VSMC_CUDA_OK; ++jf) {
+            t->tune_move = moves[im];
+            t->tune_final = finals[jf];
+            st = vsmc_cuda_cv_batch_initialize(t, m, ts.data());
+            if (st == VSMC_CUDA_OK) // the prior step, untimed
+                st = vsmc_cuda_cv_batch_step(t, m, ts.data());
+            cudaEventRecord(e0, b->stream);
+            for (int q = 0; q < 3 && st == VSMC_CUDA_OK; ++q)
+                st = vsmc_cuda_cv_batch_step(t, m, ts.data());
+            cudaEventRecord(e1, b->stream);
+            if (st != VSMC_CUDA_OK)
+                break;
+            cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_move = moves[im];
+                best_final = finals[jf];
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->launches += t->launches;
+    const int dst = vsmc_cuda_cv_batch_destroy(t);
+    if (st == VSMC_CUDA_OK)
+        st = dst;
+    if (st != VSMC_CUDA_OK)
+        return st;
+    st = vsmc_cuda_cv_batch_set_launch_shape(b, best_move, best_final);
+    if (st != VSMC_CUDA_OK)
+        return st;
+    if (move_blocks)
+        *move_blocks = b->tune_move;
+    if (final_threads)
+        *final_threads = b->tune_final;
     return VSMC_CUDA_OK;
 }
 

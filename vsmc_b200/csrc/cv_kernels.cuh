@@ -537,9 +537,11 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
     if (lane == 0)
         sh[0][wid] = m;
     __syncthreads();
+    // the warps of this launch (at most NW; a batch may launch fewer)
+    const int nwa = (int)(blockDim.x >> 5);
     if (threadIdx.x == 0) {
         double r = -INFINITY;
-        for (int w = 0; w < NW; ++w)
+        for (int w = 0; w < nwa; ++w)
             r = (sh[0][w] != sh[0][w] || r != r) ? NAN : fmax(r, sh[0][w]);
         sh_M = r;
     }
@@ -570,7 +572,7 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
     const double Nd = (double)a.N;
     if (threadIdx.x == 0) {
         double r[6] = {0, 0, 0, 0, 0, 0};
-        for (int w = 0; w < NW; ++w)
+        for (int w = 0; w < nwa; ++w)
             for (int k = 0; k < 6; ++k)
                 r[k] += sh[k][w];
         const double S1 = r[0], S2 = r[1];
