@@ -524,11 +524,23 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
     const int nt = a.ntiles;
     const bool staged = nt <= agg_cap;
     double *share = staged ? agg : a.tile_excl; // scratch when not staged
-    // pass 1: maximum (NaN propagates)
+    // pass 1: maximum (NaN propagates); a thread's tiles t, t + blockDim,
+    // ... are loaded four at a time so that their latencies overlap
+    const int bd = (int)blockDim.x;
     double m = -INFINITY;
-    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
-        const double mt = a.ts[t].m, st = a.ts[t].s1;
-        m = (mt != mt || st != st) ? NAN : (m != m ? m : fmax(m, mt));
+    for (int t0 = threadIdx.x; t0 < nt; t0 += 4 * bd) {
+        double mt[4], st[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int t = t0 + k * bd;
+            mt[k] = t < nt ? a.ts[t].m : -INFINITY; // -inf: no effect
+            st[k] = t < nt ? a.ts[t].s1 : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            m = (mt[k] != mt[k] || st[k] != st[k])
+                    ? NAN
+                    : (m != m ? m : fmax(m, mt[k]));
     }
     for (int o = 16; o > 0; o >>= 1) {
         const double q = __shfl_xor_sync(0xffffffffu, m, o);
@@ -549,17 +561,28 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
     const double M = sh_M;
     // pass 2: sums rescaled to M; shares exp(m_t - M) s1_t (unnormalised)
     double v[6] = {0, 0, 0, 0, 0, 0};
-    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
-        const TileStats ts = a.ts[t];
-        const double f = ts.m == -INFINITY ? 0.0 : exp(ts.m - M);
-        const double s1 = ts.s1 * f;
-        share[t] = s1;
-        v[0] += s1;
-        v[1] += ts.s2 * f * f;
-        v[2] += ts.sx * f;
-        v[3] += ts.sy * f;
-        v[4] += ts.gx;
-        v[5] += ts.gy;
+    for (int t0 = threadIdx.x; t0 < nt; t0 += 2 * bd) {
+        TileStats tb[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
+            if (t0 + k * bd < nt)
+                tb[k] = a.ts[t0 + k * bd];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int t = t0 + k * bd;
+            if (t < nt) {
+                const TileStats &ts = tb[k];
+                const double f = ts.m == -INFINITY ? 0.0 : exp(ts.m - M);
+                const double s1 = ts.s1 * f;
+                share[t] = s1;
+                v[0] += s1;
+                v[1] += ts.s2 * f * f;
+                v[2] += ts.sx * f;
+                v[3] += ts.sy * f;
+                v[4] += ts.gx;
+                v[5] += ts.gy;
+            }
+        }
     }
 #pragma unroll
     for (int k = 0; k < 6; ++k) {

@@ -58,20 +58,21 @@ __device__ __forceinline__ int bin_kbits(long long NN)
 
 __device__ __forceinline__ long long bin_floor(double u, int kb)
 {
-    // floor(u * K) clamped to [-1, K]
-    const double v = ldexp(u, kb);
-    const double K = ldexp(1.0, kb);
+    // floor(u * K) clamped to [-1, K]; K = 2^kb, so u * K is exact
+    const double K = (double)(1ll << kb);
+    const double v = __dmul_rn(u, K);
     if (!(v >= 0.0))
         return -1;
-    return v >= K ? (long long)K : (long long)v;
+    return v >= K ? (1ll << kb) : (long long)v;
 }
 
-__device__ __forceinline__ void bin_write(int32_t *L, int kb, double uprev,
-                                          double u, long long n, long long NN)
+// Bins (klo - 1, khi] start at u_n: klo - 1 = bin_floor(u_{n-1}) (0 for
+// n = 0), khi = bin_floor(u_n); callers carry khi on to the next n.
+__device__ __forceinline__ void bin_fill(int32_t *L, int kb, long long klo,
+                                         long long khi, long long n,
+                                         long long NN)
 {
     const long long K = 1ll << kb;
-    const long long klo = n == 0 ? 0 : bin_floor(uprev, kb) + 1;
-    long long khi = bin_floor(u, kb);
     // k/K <= u  <=>  k <= floor(u K)
     for (long long k = klo; k <= khi && k <= K; ++k)
         L[k] = (int32_t)n;
@@ -261,14 +262,33 @@ __device__ __forceinline__ void spine_scan_f64(const double *in, double *excl,
     const int b = threadIdx.x * per;
     const int e = min(b + per, ntiles);
     double run = 0.0;
-    for (int t = b; t < e; ++t)
-        run += __dmul_rn(in[t], scale);
     double total;
-    const double off = block_excl_scan(run, sh, total);
-    run = off;
-    for (int t = b; t < e; ++t) {
-        excl[t] = run;
-        run += __dmul_rn(in[t], scale);
+    if (per <= 8) {
+        // the run's loads issued together, then summed in order
+        double x[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            x[k] = b + k < e ? __dmul_rn(in[b + k], scale) : 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (b + k < e)
+                run += x[k];
+        run = block_excl_scan(run, sh, total);
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (b + k < e) {
+                excl[b + k] = run;
+                run += x[k];
+            }
+    } else {
+        for (int t = b; t < e; ++t)
+            run += __dmul_rn(in[t], scale);
+        const double off = block_excl_scan(run, sh, total);
+        run = off;
+        for (int t = b; t < e; ++t) {
+            excl[t] = run;
+            run += __dmul_rn(in[t], scale);
+        }
     }
     if (threadIdx.x == blockDim.x - 1)
         excl[ntiles] = total;
@@ -429,16 +449,18 @@ k_uniforms_stratified_body(EngineRef eng, const ResampleCtl *ctl, double *u,
     }
     if (!live)
         return;
-    // monotone sequence v_n = max(u_n, u_{n-1}); vprev = v_{n-1}
-    double vprev = fmax(p1, p2), rprev = p1;
+    // monotone sequence v_n = max(u_n, u_{n-1}); kprev = bin of v_{n-1}
+    long long kprev = bin_floor(fmax(p1, p2), kb);
+    double rprev = p1;
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
         const long long n = (long long)(b * 4 + l) - (long long)off;
         if (n >= 0 && n < NN) {
             const double v = fmax(raw[l], rprev);
             u[n] = v;
-            bin_write(L, kb, vprev, v, n, NN);
-            vprev = v;
+            const long long khi = bin_floor(v, kb);
+            bin_fill(L, kb, n == 0 ? 0 : kprev + 1, khi, n, NN);
+            kprev = khi;
         }
         rprev = raw[l];
     }
@@ -589,13 +611,16 @@ k_sorted_uniforms_body(EngineRef eng, const ResampleCtl *ctl,
         exc = fmax(exc, shm[w]);
     double m = fmax(umax, exc);
     const int kb = ctl->kbits;
+    long long kprev = bin_floor(m, kb); // bin of u_{n-1}
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-        const double prevm = m;
         m = fmax(m, uv[j]);
-        if (n0 + j < NN) {
-            u[n0 + j] = m;
-            bin_write(L, kb, prevm, m, n0 + j, NN);
+        const long long n = n0 + j;
+        if (n < NN) {
+            u[n] = m;
+            const long long khi = bin_floor(m, kb);
+            bin_fill(L, kb, n == 0 ? 0 : kprev + 1, khi, n, NN);
+            kprev = khi;
         }
     }
 }
@@ -638,6 +663,24 @@ __device__ __forceinline__ int first_above_shared(const int32_t *s, int n,
             l = m + 1;
     }
     return l;
+}
+
+// The same count for a query C >= the previous query of this thread, whose
+// count was `c`: gallop from c (probes c, c+1, c+3, c+7, ...) and finish
+// with a binary search inside the last gap, so a query that passes k values
+// costs about 2 log2(k + 1) probes instead of log2(n).
+__device__ __forceinline__ int ub_gallop(const double *u, int c, int n,
+                                         double C)
+{
+    int lo = c, step = 1;
+    while (lo < n) {
+        const int p = min(lo + step - 1, n - 1);
+        if (u[p] > C)
+            return ub_shared(u, lo, p, C);
+        lo = p + 1;
+        step <<= 1;
+    }
+    return n;
 }
 
 __device__ __forceinline__ long long ub_global(const double *u, long long lo,
@@ -797,86 +840,95 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
             sw[n - lo] = u[n];
     __syncthreads();
 
-    // counts c_i = #{n: u_n <= C_i} for this thread's particles
-    long long cnt[kItems];
-    long long k_int[kItems];
+    // counts c_i = #{n: u_n <= C_i} for this thread's particles; C_i is
+    // non-decreasing along the thread's particles, so after the first
+    // search each count gallops on from the previous one.  Counts, indices
+    // and prefixes are 32-bit: N <= 2^30.
+    const int ilo = (int)lo, ihi = (int)hi, iNN = (int)NN, iN = (int)N;
+    const int i0 = (int)base + (int)threadIdx.x * kItems;
+    int cnt[kItems];
+    int k_int[kItems];
+    int pos = -1;
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-        const long long i = base + (long long)threadIdx.x * kItems + j;
+        const int i = i0 + j;
         pre += wv[j];
         double C = fmin(__dadd_rn(a, pre), b);
-        if (i == base + kTile - 1 || i == N - 1)
+        if (i == (int)base + kTile - 1 || i == iN - 1)
             C = b;
-        long long c;
-        if (i >= N - 1) {
-            c = NN; // the last particle takes every remaining uniform
+        int c;
+        if (i >= iN - 1) {
+            c = iNN; // the last particle takes every remaining uniform
         } else if (Sys) {
-            c = sys_count(C, u0, delta, NN);
+            c = (int)sys_count(C, u0, delta, NN);
         } else if (staged) {
-            c = lo + ub_shared(sw, 0, (int)(hi - lo), C);
+            pos = pos < 0 ? ub_shared(sw, 0, ihi - ilo, C)
+                          : ub_gallop(sw, pos, ihi - ilo, C);
+            c = ilo + pos;
         } else {
-            c = ub_global(u, lo, hi, C);
+            c = (int)ub_global(u, lo, hi, C);
         }
-        cnt[j] = min(max(c, lo), i >= N - 1 ? NN : hi);
-        k_int[j] = Residual ? (long long)sk[threadIdx.x * kItems + j] : 0;
+        cnt[j] = min(max(c, ilo), i >= iN - 1 ? iNN : ihi);
+        k_int[j] = Residual ? (int)sk[threadIdx.x * kItems + j] : 0;
     }
 #pragma unroll
     for (int j = 1; j < kItems; ++j)
         cnt[j] = max(cnt[j], cnt[j - 1]);
-    long long prev = __shfl_up_sync(0xffffffffu, cnt[kItems - 1], 1);
+    int prev = __shfl_up_sync(0xffffffffu, cnt[kItems - 1], 1);
     if ((threadIdx.x & 31) == 31)
         sh_last[wid] = cnt[kItems - 1];
     __syncthreads();
     if ((threadIdx.x & 31) == 0)
-        prev = (threadIdx.x == 0) ? (tile > 0 ? lo : 0) : sh_last[wid - 1];
-    long long rep[kItems];
+        prev = (threadIdx.x == 0) ? (tile > 0 ? ilo : 0)
+                                  : (int)sh_last[wid - 1];
+    int rep[kItems];
     int zeros = 0;
-    long long ksum = 0;
+    int ksum = 0;
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-        const long long i = base + (long long)threadIdx.x * kItems + j;
-        const long long c = max(cnt[j], prev);
-        rep[j] = (i < N) ? (c - prev) + k_int[j] : 0;
+        const int i = i0 + j;
+        const int c = max(cnt[j], prev);
+        rep[j] = (i < iN) ? (c - prev) + k_int[j] : 0;
         prev = c;
         cnt[j] = c;
-        zeros += (i < N && rep[j] == 0) ? 1 : 0;
+        zeros += (i < iN && rep[j] == 0) ? 1 : 0;
         ksum += k_int[j];
     }
     // the last queried uniform fixes the words drawn (inversion queries
     // u_0..u_{n_final}, common.hpp:76-81)
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-        const long long i = base + (long long)threadIdx.x * kItems + j;
-        if (i == N - 2) {
+        if (i0 + j == iN - 2) {
             ctl->n_final = cnt[j];
             if (!Sys)
-                ctl->words = (NN > 0) ? (unsigned long long)min(NN, cnt[j] + 1)
+                ctl->words = (NN > 0) ? (unsigned long long)min(iNN, cnt[j] + 1)
                                       : 0ull;
         }
     }
-    long long ztot;
-    long long zloc = block_excl_scan((long long)zeros, shl, ztot);
-    long long ktot;
-    const long long kex = Residual ? block_excl_scan(ksum, shl, ktot) : 0;
+    int *shi = reinterpret_cast<int *>(shl);
+    int ztot;
+    int zloc = block_excl_scan(zeros, shi, ztot);
+    int ktot;
+    const int kex = Residual ? block_excl_scan(ksum, shi, ktot) : 0;
     if (threadIdx.x == 0)
-        tile_zeros[tile] = (int32_t)ztot;
-    const long long tile_last = min(base + (long long)kTile, N) - 1;
-    long long kprefix = Residual ? tile_kexcl[tile] + kex : 0;
+        tile_zeros[tile] = ztot;
+    const int tile_last = (int)min(base + (long long)kTile, N) - 1;
+    int kprefix = Residual ? (int)tile_kexcl[tile] + kex : 0;
     int32_t cf[kItems], sc[kItems], rp[kItems];
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-        const long long i = base + (long long)threadIdx.x * kItems + j;
+        const int i = i0 + j;
         kprefix += k_int[j];
         // R_{<=i} = count_i + K_{<=i}; the last particle closes at N
-        const long long R = (i >= N - 1) ? N : cnt[j] + kprefix;
+        const int R = (i >= iN - 1) ? iN : cnt[j] + kprefix;
         if (rep[j] == 0) {
-            cf[j] = (int32_t)(-(zloc + 1));
+            cf[j] = -(zloc + 1);
             ++zloc;
         } else {
-            cf[j] = (int32_t)i;
+            cf[j] = i;
         }
-        sc[j] = (int32_t)(R - (i + 1) + zloc);
-        rp[j] = (int32_t)rep[j];
+        sc[j] = R - (i + 1) + zloc;
+        rp[j] = rep[j];
         if (i == tile_last)
             tile_sinc_last[tile] = sc[j];
     }
@@ -941,7 +993,8 @@ struct SmemZeroSpine {
     int32_t S[kSpineStage]; // zero counts, then surplus ends E
 };
 struct SmemFill {
-    int32_t ss[kTile];
+    int32_t ss[kTile];  // sinc of one parent tile
+    int32_t tab[kTile]; // parent of each zero-slot rank of this tile
 };
 
 __device__ __forceinline__ void
@@ -957,6 +1010,7 @@ k_zero_spine_body(const int32_t *tile_zeros, const int32_t *tile_sinc_last,
     // phase 1: exclusive prefix of the zero counts (striped load, ordered
     // contiguous runs from shared memory)
     if (staged) {
+#pragma unroll 8
         for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
             S[t] = tile_zeros[t];
         __syncthreads();
@@ -980,6 +1034,7 @@ k_zero_spine_body(const int32_t *tile_zeros, const int32_t *tile_sinc_last,
     __syncthreads();
     // phase 2: E[t] = surplus count at the end of tile t (non-decreasing)
     if (staged) {
+#pragma unroll 8
         for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
             S[t] = tile_sinc_last[t] + zexcl[t];
         __syncthreads();
@@ -1026,8 +1081,11 @@ k_zero_spine(const int32_t *tile_zeros, const int32_t *tile_sinc_last,
 // internal::cfrp_trans for the slots without offspring (common.hpp:94-106):
 // the k-th such slot takes the k-th surplus child in parent order, i.e. the
 // first parent p with sinc(p) > k, sinc(p) = sinc_local[p] + zexcl[tile(p)].
-// The CTA of tile t stages the parent tiles tfirst[t]..tlast[t] one at a
-// time in shared memory; every slot binary-searches its parent there.
+// The zero slots of tile t hold the consecutive ranks [zexcl[t],
+// zexcl[t + 1]).  The CTA of tile t stages the parent tiles tfirst[t]..
+// tlast[t] one at a time in shared memory; parent p owns the ranks
+// [sinc(p - 1), sinc(p)) and writes itself into a rank -> parent table for
+// those that fall in the tile's window, so no slot searches.
 __device__ __forceinline__ void
 k_cfrp_fill_body(long long N, ResampleCtl *ctl, const int32_t *sinc_local,
                  const int32_t *zexcl, const int32_t *tfirst,
@@ -1037,25 +1095,23 @@ k_cfrp_fill_body(long long N, ResampleCtl *ctl, const int32_t *sinc_local,
     if (!ctl->active)
         return;
     int32_t *ss = sm.ss;
+    int32_t *tab = sm.tab;
     const int tile = tile_bid;
     const int t0 = tfirst[tile], t1 = tlast[tile];
     if (t1 < t0)
         return; // every particle of the tile has offspring
-    const long long Z0 = zexcl[tile];
+    const int Z0 = zexcl[tile];
+    const int z = min(zexcl[tile + 1] - Z0, kTile); // zero slots of the tile
     const long long base = (long long)tile * kTile;
-    long long rank[kItems];
-    int32_t parent[kItems];
+    int32_t cf[kItems];
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
         const long long i = base + (long long)j * kThreads + threadIdx.x;
-        rank[j] = -1;
-        parent[j] = 0;
-        if (i < N) {
-            const int32_t c = copy_from[i];
-            if (c < 0)
-                rank[j] = Z0 + (long long)(-c) - 1;
-        }
+        cf[j] = i < N ? copy_from[i] : 0;
     }
+    for (int k = threadIdx.x; k < z; k += kThreads)
+        tab[k] = -1;
+    int prev_top = INT_MIN; // ranks below the first staged tile map to it
     for (int pt = t0; pt <= t1; ++pt) {
         const long long pb = (long long)pt * kTile;
         const int len = (int)min((long long)kTile, N - pb);
@@ -1063,25 +1119,27 @@ k_cfrp_fill_body(long long N, ResampleCtl *ctl, const int32_t *sinc_local,
         for (int j = threadIdx.x; j < len; j += kThreads)
             ss[j] = sinc_local[pb + j] + zoff;
         __syncthreads();
-        const long long top = ss[len - 1];
-#pragma unroll
-        for (int j = 0; j < kItems; ++j) {
-            if (rank[j] >= 0 && rank[j] < top) {
-                parent[j] =
-                    (int32_t)(pb + first_above_shared(ss, len, rank[j]));
-                rank[j] = -2;
-            }
+        for (int j = threadIdx.x; j < len; j += kThreads) {
+            const int lo = max(j > 0 ? ss[j - 1] : prev_top, Z0);
+            const int hi = min(ss[j], Z0 + z);
+            for (int r = lo; r < hi; ++r)
+                tab[r - Z0] = (int32_t)(pb + j);
         }
+        prev_top = max(prev_top, ss[len - 1]);
         __syncthreads();
     }
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
         const long long i = base + (long long)j * kThreads + threadIdx.x;
-        if (rank[j] == -2) {
-            copy_from[i] = parent[j];
-        } else if (rank[j] >= 0) { // no parent found: replication != N
-            atomicExch(&ctl->error, (int)VSMC_CUDA_EDEGENERATE);
-            copy_from[i] = (int32_t)i;
+        if (i < N && cf[j] < 0) {
+            const int k = -cf[j] - 1; // rank - Z0
+            const int32_t p = k < z ? tab[k] : -1;
+            if (p >= 0) {
+                copy_from[i] = p;
+            } else { // no parent found: replication != N
+                atomicExch(&ctl->error, (int)VSMC_CUDA_EDEGENERATE);
+                copy_from[i] = (int32_t)i;
+            }
         }
     }
 }
@@ -1161,13 +1219,15 @@ k_apply_max(const double *u, long long n, const double *tile_max, double *out,
     double m = fmax(carry_sh, threadIdx.x > 0 ? shm[threadIdx.x - 1]
                                               : -INFINITY);
     const int kb = ctl->kbits;
+    long long kprev = bin_floor(m, kb);
     for (int j = 0; j < kItems; ++j) {
         const long long i = base + (long long)threadIdx.x * kItems + j;
-        const double prevm = m;
         m = fmax(m, v[j]);
         if (i < n) {
             out[i] = m;
-            bin_write(L, kb, prevm, m, i, n);
+            const long long khi = bin_floor(m, kb);
+            bin_fill(L, kb, i == 0 ? 0 : kprev + 1, khi, i, n);
+            kprev = khi;
         }
     }
 }
