@@ -524,6 +524,29 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
     const int nt = a.ntiles;
     const bool staged = nt <= agg_cap;
     double *share = staged ? agg : a.tile_excl; // scratch when not staged
+    // thread 0's reads of the control block and observations, issued
+    // before the passes so that its serial section does not wait on them
+    FilterCtl *c = a.ctl;
+    int c_res = 0, rflag = 0;
+    long long c_mdone = 0;
+    double c_s1 = 0.0, c_logz = 0.0;
+    double ax0 = 0.0, ay0 = 0.0, ax1 = 0.0, ay1 = 0.0;
+    if (threadIdx.x == 0) {
+        c_res = c->resampled;
+        c_mdone = c->monitor_done;
+        c_s1 = c->s1;
+        c_logz = c->logz;
+        if (a.anchored) {
+            if (!a.init) {
+                ax0 = a.obs_x[a.t - 1];
+                ay0 = a.obs_y[a.t - 1];
+            }
+            ax1 = a.obs_x[a.t];
+            ay1 = a.obs_y[a.t];
+        }
+        if (a.replay_flags != nullptr)
+            rflag = a.replay_flags[a.t];
+    }
     // pass 1: maximum (NaN propagates); a thread's tiles t, t + blockDim,
     // ... are loaded four at a time so that their latencies overlap
     const int bd = (int)blockDim.x;
@@ -591,7 +614,6 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
             sh[k][wid] = v[k];
     }
     __syncthreads();
-    FilterCtl *c = a.ctl;
     const double Nd = (double)a.N;
     if (threadIdx.x == 0) {
         double r[6] = {0, 0, 0, 0, 0, 0};
@@ -600,14 +622,12 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
                 r[k] += sh[k][w];
         const double S1 = r[0], S2 = r[1];
         // monitor of the previous step, gathered by this move
-        if (!a.init && c->resampled && c->monitor_done != a.t - 1) {
-            const double ax = a.anchored ? a.obs_x[a.t - 1] : 0.0;
-            const double ay = a.anchored ? a.obs_y[a.t - 1] : 0.0;
-            a.hist_mean_x[a.t - 1] = ax + r[4] / Nd;
-            a.hist_mean_y[a.t - 1] = ay + r[5] / Nd;
+        if (!a.init && c_res && c_mdone != a.t - 1) {
+            a.hist_mean_x[a.t - 1] = ax0 + r[4] / Nd;
+            a.hist_mean_y[a.t - 1] = ay0 + r[5] / Nd;
             c->monitor_done = a.t - 1;
         }
-        const double s1prev = (a.init || c->resampled) ? Nd : c->s1;
+        const double s1prev = (a.init || c_res) ? Nd : c_s1;
         int res = 0;
         double ess = S1 * S1 / S2;
         double dz = M + log(S1) - log(s1prev);
@@ -620,21 +640,19 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
             res = ess < a.threshold * Nd;
         }
         if (a.replay_flags != nullptr)
-            res = a.replay_flags[a.t] != 0;
+            res = rflag != 0;
         a.hist_ess[a.t] = ess;
         a.hist_resampled[a.t] = res;
         a.hist_logz_inc[a.t] = dz;
-        c->logz += dz;
+        c->logz = c_logz + dz;
         c->lw_max = M;
         c->s1 = S1;
         c->s2 = S2;
         c->ess = ess;
         c->resampled = res;
         if (!res) {
-            const double ax = a.anchored ? a.obs_x[a.t] : 0.0;
-            const double ay = a.anchored ? a.obs_y[a.t] : 0.0;
-            a.hist_mean_x[a.t] = ax + r[2] / S1;
-            a.hist_mean_y[a.t] = ay + r[3] / S1;
+            a.hist_mean_x[a.t] = ax1 + r[2] / S1;
+            a.hist_mean_y[a.t] = ay1 + r[3] / S1;
         }
         a.rctl->active = a.replay_flags != nullptr ? 0 : res;
         sh_res = a.replay_flags != nullptr ? 0 : res;
@@ -652,14 +670,20 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
         run += share[t] * coeff;
     double total;
     double off = block_excl_scan(run, sh_spine, total);
-    // in place when the shares live in tile_excl: read before write per t
+    // in place in `share` (read before write per t); staged shares are then
+    // copied out with coalesced stores
     for (int t = b; t < e; ++t) {
         const double x = share[t] * coeff;
-        a.tile_excl[t] = off;
+        share[t] = off;
         off += x;
     }
     if (threadIdx.x == blockDim.x - 1)
         a.tile_excl[nt] = total;
+    if (staged) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < nt; t += bd)
+            a.tile_excl[t] = share[t];
+    }
     if (threadIdx.x == 0) {
         ResampleCtl *rc = a.rctl;
         rc->NN = a.N;

@@ -823,6 +823,19 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
             sk[l] = k;
     }
     __syncthreads();
+    // the tile's uniforms are loaded into registers now and written to
+    // shared memory after the scan, so their latency overlaps the scan
+    const long long lo = sh_bound[0];
+    const long long hi = max(sh_bound[1], lo);
+    const bool staged = !Sys && (hi - lo) <= kUStage;
+    double upre[kUStage / kThreads];
+    if (staged) {
+#pragma unroll
+        for (int j = 0; j < kUStage / kThreads; ++j) {
+            const long long n = lo + j * kThreads + threadIdx.x;
+            upre[j] = n < hi ? u[n] : 0.0;
+        }
+    }
     double wv[kItems];
     double run = 0.0;
 #pragma unroll
@@ -832,12 +845,14 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     }
     double total;
     double pre = block_excl_scan(run, shd, total); // ends with a barrier
-    const long long lo = sh_bound[0];
-    const long long hi = max(sh_bound[1], lo);
-    const bool staged = !Sys && (hi - lo) <= kUStage;
-    if (staged)
-        for (long long n = lo + threadIdx.x; n < hi; n += kThreads)
-            sw[n - lo] = u[n];
+    if (staged) {
+#pragma unroll
+        for (int j = 0; j < kUStage / kThreads; ++j) {
+            const long long n = lo + j * kThreads + threadIdx.x;
+            if (n < hi)
+                sw[n - lo] = upre[j];
+        }
+    }
     __syncthreads();
 
     // counts c_i = #{n: u_n <= C_i} for this thread's particles; C_i is
