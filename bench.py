@@ -202,6 +202,39 @@ def forms_compare(capi, N, sch, K, W, ox, oy, sp, fp64_step_ms):
                             "copy_from vectors (fixed ancestry) over the same T steps"}
 
 
+def scheme_sweep(capi, sp, sizes=(1 << 16, 1 << 20, 1 << 24), K=20, W=3,
+                 cpu=True):
+    """Every resampling scheme at N = 2^16, 2^20, 2^24 in both forms: device
+    time per step and per move from the library's own CUDA events on the
+    filter's stream, over K steps after W warm-up steps of the same filter
+    (T = 1 + W + K).  The vSMC reference (StateOMP, all host threads) runs
+    the same filter on the host for N <= 2^20."""
+    rows = []
+    T = 1 + W + K
+    ox, oy = capi.cv_simulate(T, OBS_SEED)
+    for N in sizes:
+        for sch, name in enumerate(SCHEMES):
+            row = {"N": N, "scheme": name}
+            for form, fname in ((capi.FP64, "fp64"), (capi.MIXED, "mixed")):
+                with capi.CVFilter(N, T, scheme=sch, form=form, seed=101, stream=sp) as f:
+                    f.set_observations_host(ox, oy)
+                    f.initialize()
+                    f.iterate(W)
+                    f.set_timing(True)
+                    f.iterate(K)
+                    mv_ms, st_ms, n, _ = f.timing()
+                    h = f.history()
+                row[fname] = {"ms_per_step": st_ms / n, "move_ms": mv_ms / n,
+                              "particle_steps_per_s": N / (st_ms / n / 1e3),
+                              "resampled_steps": int(sum(h["resampled"][1 + W:T]))}
+            if cpu and N <= 1 << 20:
+                v, info = cpu_reference(N, sch, 0, 0, sample_steps=6)
+                row["cpu_reference"] = {"particle_steps_per_s": v, "cores": info["cores"],
+                                        "kind": info["kind"]}
+            rows.append(row)
+    return rows
+
+
 def batched_workload(capi, n_filters=4096, seed=2024):
     """4096 filters: N log-uniform on [2^10, 2^16], T uniform on [50, 500],
     each with its own simulated series (obs seed 1000 + k, stream k)."""
@@ -550,6 +583,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_extras:
         if args.form == "fp64":
             extras["forms"] = forms_compare(capi, N, sch, K, W, ox, oy, sp, ms / K)
+        extras["schemes"] = {
+            "workload": "CV Student-t filter, each scheme at N = 2^16, 2^20, 2^24, threshold "
+                        "0.5, 20 timed steps after 3 warm-up steps",
+            "points": scheme_sweep(capi, sp, cpu=not args.no_cpu_baseline)}
         bN, bT, bobs = batched_workload(capi)
         extras["batched"] = {
             "workload": "4096 CV Student-t filters, N log-uniform [2^10, 2^16], T uniform "

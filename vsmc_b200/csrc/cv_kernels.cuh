@@ -59,15 +59,18 @@ struct MoveArgs {
 
 template <typename Real>
 struct Vec;
+// Particles per thread per pass: FP64 one (scalar loads keep the move at
+// 80 registers without spills), float two (float2); both measured faster
+// than double2 / float4.
 template <>
 struct Vec<double> {
-    static constexpr int n = 2;
-    typedef double2 type;
+    static constexpr int n = 1;
+    typedef double type;
 };
 template <>
 struct Vec<float> {
-    static constexpr int n = 4;
-    typedef float4 type;
+    static constexpr int n = 2;
+    typedef float2 type;
 };
 
 __device__ __forceinline__ double plus0(double v) { return __dadd_rn(v, 0.0); }
