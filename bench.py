@@ -263,7 +263,7 @@ def batched_run(capi, form, N, T, obs, reps=3, autotune=True):
     with capi.CVBatch(nf, scheme=0, form=form, stream=stream.cuda_stream) as b:
         slots = [b.admit(int(N[k]), int(T[k]), 101 + k, k) for k in range(nf)]
         b.set_observations(slots, obs)
-        shape = b.autotune(slots) if autotune else (3, 1024)
+        shape = b.autotune(slots) if autotune else (4, 256)
         b.run(slots)
         b.synchronize()
         dev_ms = []

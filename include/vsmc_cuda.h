@@ -382,7 +382,7 @@ int vsmc_cuda_cv_batch_set_graphs(vsmc_cuda_cv_batch *b, int enable);
  * (2, 3 or 4) CTAs per SM, the finalize CTA at `final_threads` (1024 or
  * 256; 256 applies only while every admitted filter has at most 256 tiles
  * of 2048 particles).  No shape changes a result.  New batches start at
- * (3, 1024). */
+ * (4, 256). */
 int vsmc_cuda_cv_batch_set_launch_shape(vsmc_cuda_cv_batch *b,
                                         int move_blocks, int final_threads);
 

@@ -119,6 +119,26 @@ def test_invariants_and_determinism(capi, sch):
     assert np.array_equal(np.bincount(cf, minlength=N), rep)
 
 
+@pytest.mark.parametrize("stride", [3001, 40000])
+@pytest.mark.parametrize("sch", [0, 3, 4])
+def test_sparse_parents_against_oracle(capi, stride, sch):
+    """Weight only on every stride-th particle (and the last one): each
+    parent has thousands of children, so the empty slots of one tile take
+    their parents from other tiles, up to tens of tiles away."""
+    N = (1 << 17) + 5
+    rng = np.random.default_rng(stride + sch)
+    w = np.zeros(N)
+    w[::stride] = rng.uniform(0.5, 1.5, size=len(w[::stride]))
+    w[-1] = 1.0
+    w /= w.sum()
+    ref_rep, ref_cf, ref_words, uni = O.resample(sch, w, 29, 1, want_uniforms=True)
+    rep, cf, words = gpu_resample(capi, sch, w, 29, 1,
+                                  uni if sch in LOG_EXP_SCHEMES else None)
+    assert words == ref_words
+    assert np.array_equal(rep, ref_rep)
+    assert np.array_equal(cf, ref_cf)
+
+
 def test_degenerate_and_equal_weights(capi):
     N = 1 << 16
     w = np.zeros(N)

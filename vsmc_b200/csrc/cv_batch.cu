@@ -770,8 +770,10 @@ int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
     b->obs_cap = 0;
     b->launches = 0;
     b->use_graphs = true;
-    b->tune_move = 3;
-    b->tune_final = kFinalThreads;
+    // the autotuner's usual pick on mixed workloads; 256-thread finalize
+    // applies only while every filter has at most 256 tiles
+    b->tune_move = 4;
+    b->tune_final = 256;
     b->max_ntiles = 0;
     b->run_exec = nullptr;
     b->run_map = nullptr;
