@@ -353,6 +353,18 @@ int vsmc_cuda_cv_batch_step(vsmc_cuda_cv_batch *b, uint32_t n,
 int vsmc_cuda_cv_batch_run(vsmc_cuda_cv_batch *b, uint32_t n,
                            const uint32_t *slots);
 
+/* The last counts[k] steps of each listed slot, oldest first, packed in
+ * list order (sum of counts entries per array): ESS, log-evidence
+ * increment, resampled flag; status[k] is the slot's sticky device status
+ * (host arrays; each may be NULL).  The running log-evidence after a step is
+ * the previous one plus its increment, in that order (the device's own sum).
+ * Synchronises; returns the first non-zero status. */
+int vsmc_cuda_cv_batch_read_steps(vsmc_cuda_cv_batch *b, uint32_t n,
+                                  const uint32_t *slots,
+                                  const uint32_t *counts, double *ess,
+                                  double *logz_inc, int32_t *resampled,
+                                  int32_t *status);
+
 /* The last step of each listed slot: ESS, log-evidence increment,
  * resampled flag, running log-evidence and the slot's sticky device status
  * (host arrays of n; each may be NULL).  Synchronises; returns the first

@@ -244,3 +244,44 @@ def test_batch_launch_shape_rejects(capi):
         for shape in ((1, 1024), (5, 1024), (3, 512)):
             with pytest.raises(capi.VsmcCudaError):
                 b.set_launch_shape(*shape)
+
+
+def test_batch_read_steps(golden, capi):
+    """Several observations appended per slot, one run through them all:
+    read_steps gives each slot's last steps exactly as its history has them,
+    and the running log-evidence is the sequential sum of the increments."""
+    specs = SPECS[:5]
+    obs = [series(capi, golden, k, T, sid) for k, (N, T, seed, sid) in enumerate(specs)]
+    with capi.CVBatch(len(specs), scheme=0, form=0) as b:
+        slots = [b.admit(N, T, seed, sid) for (N, T, seed, sid) in specs]
+        pos = [0] * len(specs)
+        rng = np.random.default_rng(5)
+        while any(pos[k] < specs[k][1] for k in range(len(specs))):
+            counts = [min(int(rng.integers(1, 5)), specs[k][1] - pos[k]) for k in range(len(specs))]
+            live = [k for k in range(len(specs)) if counts[k] > 0]
+            for j in range(max(counts)):
+                rnd = [k for k in live if counts[k] > j]
+                b.append_observations([slots[k] for k in rnd],
+                                      [obs[k][0][pos[k] + j] for k in rnd],
+                                      [obs[k][1][pos[k] + j] for k in rnd])
+            b.run([slots[k] for k in live])
+            got = b.read_steps([slots[k] for k in live], [counts[k] for k in live])
+            off = 0
+            for k in live:
+                h = b.history(slots[k])
+                sl = slice(pos[k], pos[k] + counts[k])
+                g = slice(off, off + counts[k])
+                assert np.array_equal(got["ess"][g], h["ess"][sl]), k
+                assert np.array_equal(got["logz_inc"][g], h["logz_inc"][sl]), k
+                assert np.array_equal(got["resampled"][g], h["resampled"][sl]), k
+                off += counts[k]
+                pos[k] += counts[k]
+            assert np.all(got["status"] == 0)
+        last = b.read_last(slots)
+    for k, (N, T, seed, sid) in enumerate(specs):
+        s = single(capi, N, T, 0, 0, seed, sid, *obs[k])
+        assert last["log_evidence"][k] == np.cumsum(s["logz_inc"])[-1]
+    with capi.CVBatch(1) as b:
+        s0 = b.admit(1000, 4)
+        with pytest.raises(capi.VsmcCudaError):
+            b.read_steps([s0], [1])  # no step taken yet

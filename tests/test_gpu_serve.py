@@ -148,3 +148,36 @@ def test_server_bad_calls(capi):
         srv.drain(10000)
         res = srv.poll()
         assert res.size == 2 and np.all(res["status"] == 0)
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_server_catch_up(capi, form):
+    """Every observation of every request is submitted at once: the loop
+    catches up several steps per request per tick (fewer ticks than steps),
+    and every per-observation result still equals the filter run alone."""
+    specs = SPECS[:6]
+    obs = [capi.cv_simulate(T, obs_seed=400 + k, stream_id=sid)
+           for k, (N, T, seed, sid) in enumerate(specs)]
+    with capi.CVServer(16, scheme=3, form=form) as srv:
+        ids = [srv.open(N, T, seed, sid) for (N, T, seed, sid) in specs]
+        Tmax = max(T for _, T, _, _ in specs)
+        for t in range(Tmax):
+            live = [k for k in range(len(specs)) if t < specs[k][1]]
+            srv.observe([ids[k] for k in live], [obs[k][0][t] for k in live],
+                        [obs[k][1][t] for k in live])
+        for k in range(len(specs)):
+            srv.close(ids[k])
+        res = collect(srv, sum(T for _, T, _, _ in specs))
+        srv.drain(10000)
+        st = srv.stats()
+    assert st["steps"] == res.size
+    assert st["ticks"] < res.size
+    assert np.all(res["status"] == 0)
+    for k, (N, T, seed, sid) in enumerate(specs):
+        r = np.sort(res[res["request"] == ids[k]], order="t")
+        assert np.array_equal(r["t"], np.arange(T))
+        h = alone(capi, N, T, seed, sid, *obs[k], 3, form)
+        assert np.array_equal(r["ess"], h["ess"]), k
+        assert np.array_equal(r["logz_inc"], h["logz_inc"]), k
+        assert np.array_equal(r["resampled"], h["resampled"]), k
+        assert np.array_equal(r["log_evidence"], np.cumsum(h["logz_inc"])), k

@@ -133,6 +133,7 @@ def lib():
     L.vsmc_cuda_cv_batch_launches.argtypes = [vp, C.POINTER(u64)]
     L.vsmc_cuda_cv_batch_set_graphs.argtypes = [vp, i32]
     L.vsmc_cuda_cv_batch_set_launch_shape.argtypes = [vp, C.c_int, C.c_int]
+    L.vsmc_cuda_cv_batch_read_steps.argtypes = [vp, u32, vp, vp, vp, vp, vp, vp]
     L.vsmc_cuda_cv_batch_autotune.argtypes = [vp, u32, vp, C.POINTER(C.c_int),
                                               C.POINTER(C.c_int)]
     L.vsmc_cuda_cv_server_create.argtypes = [C.POINTER(CVConfig), u32, u64, C.POINTER(vp)]
@@ -536,6 +537,24 @@ class CVBatch:
 
     def synchronize(self):
         check(lib().vsmc_cuda_cv_batch_synchronize(self.h), "vsmc_cuda_cv_batch_synchronize")
+
+    def read_steps(self, slots, counts):
+        """The last counts[k] steps of each slot, packed in list order:
+        dict of ess, logz_inc, resampled (sum(counts)) and status (n)."""
+        import numpy as np
+
+        a, n = self._slots(slots)
+        c = np.ascontiguousarray(counts, dtype=np.uint32)
+        tot = int(c.sum())
+        out = {"ess": np.empty(tot), "logz_inc": np.empty(tot),
+               "resampled": np.empty(tot, np.int32), "status": np.empty(n, np.int32)}
+        rc = lib().vsmc_cuda_cv_batch_read_steps(
+            self.h, n, a.ctypes.data, c.ctypes.data, out["ess"].ctypes.data,
+            out["logz_inc"].ctypes.data, out["resampled"].ctypes.data,
+            out["status"].ctypes.data)
+        if rc not in (OK, EDEGENERATE):
+            check(rc, "vsmc_cuda_cv_batch_read_steps")
+        return out
 
     def set_launch_shape(self, move_blocks, final_threads):
         check(lib().vsmc_cuda_cv_batch_set_launch_shape(self.h, move_blocks, final_threads),

@@ -332,6 +332,26 @@ static __global__ void kb_scatter_obs(const BatchSlot *slots,
     }
 }
 
+// The last `count` steps of each record's slot (index = first step): ess,
+// log-evidence increment, resampled flag packed at `src`; the slot's error
+// code per record.
+static __global__ void kb_read_steps(const BatchSlot *slots,
+                                     const ObsRecord *rec, double *out,
+                                     double *err)
+{
+    const ObsRecord r = rec[blockIdx.x];
+    const BatchSlot &b = slots[r.slot];
+    for (int k = threadIdx.x; k < r.count; k += blockDim.x) {
+        double *o = out + 3 * (r.src + k);
+        o[0] = b.hist_ess[r.index + k];
+        o[1] = b.hist_logz_inc[r.index + k];
+        o[2] = (double)b.hist_resampled[r.index + k];
+    }
+    if (threadIdx.x == 0)
+        err[blockIdx.x] =
+            (double)(b.ctl->error != 0 ? b.ctl->error : b.rws.ctl->error);
+}
+
 // Summary of each work item's last step: ess, log-evidence increment,
 // resampled flag, running log-evidence, error code.
 static __global__ void kb_read_last(const BatchSlot *slots,
@@ -442,6 +462,10 @@ struct vsmc_cuda_cv_batch {
     BatchSlot *h_slot; // pinned staging of one slot record
     double *d_out;
     double *h_out;
+    // per-step read-back (vsmc_cuda_cv_batch_read_steps), grown on demand
+    double *d_steps;
+    double *h_steps;
+    size_t steps_cap; // steps, 3 doubles each
     uint64_t launches;
     // graph of the last run (vsmc_cuda_cv_batch_run)
     bool use_graphs;
@@ -769,6 +793,9 @@ int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
     b->d_obs = nullptr;
     b->obs_cap = 0;
     b->launches = 0;
+    b->d_steps = nullptr;
+    b->h_steps = nullptr;
+    b->steps_cap = 0;
     b->use_graphs = true;
     // the autotuner's usual pick on mixed workloads; 256-thread finalize
     // applies only while every filter has at most 256 tiles
@@ -852,6 +879,8 @@ int vsmc_cuda_cv_batch_destroy(vsmc_cuda_cv_batch *b)
     cudaFree(b->d_work);
     cudaFree(b->d_rec);
     cudaFree(b->d_out);
+    cudaFree(b->d_steps);
+    cudaFreeHost(b->h_steps);
     cudaFreeHost(b->h_work);
     cudaFreeHost(b->h_rec);
     cudaFreeHost(b->h_obs);
@@ -1208,6 +1237,102 @@ int vsmc_cuda_cv_batch_run(vsmc_cuda_cv_batch *b, uint32_t n,
         e = cudaGetLastError();
     return e == cudaSuccess ? VSMC_CUDA_OK
                             : cuda_status(e, "vsmc_cuda_cv_batch_run");
+}
+
+int vsmc_cuda_cv_batch_read_steps(vsmc_cuda_cv_batch *b, uint32_t n,
+                                  const uint32_t *slots,
+                                  const uint32_t *counts, double *ess,
+                                  double *logz_inc, int32_t *resampled,
+                                  int32_t *status)
+{
+    int st = check_slots(b, n, slots, "vsmc_cuda_cv_batch_read_steps");
+    if (st != VSMC_CUDA_OK)
+        return st;
+    if (n == 0)
+        return VSMC_CUDA_OK;
+    if (counts == nullptr) {
+        set_last_error("vsmc_cuda_cv_batch_read_steps: null counts");
+        return VSMC_CUDA_EINVAL;
+    }
+    size_t total = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        if (counts[k] == 0 || counts[k] > b->t[slots[k]]) {
+            set_last_error("vsmc_cuda_cv_batch_read_steps: slot " +
+                           std::to_string(slots[k]) + " has not taken " +
+                           std::to_string(counts[k]) + " steps");
+            return VSMC_CUDA_EINVAL;
+        }
+        total += counts[k];
+    }
+    cudaError_t e = cudaSuccess;
+    if (total > b->steps_cap) {
+        e = cudaStreamSynchronize(b->stream); // old buffers may be in use
+        cudaFree(b->d_steps);
+        cudaFreeHost(b->h_steps);
+        b->d_steps = nullptr;
+        b->h_steps = nullptr;
+        b->steps_cap = 0;
+        const size_t cap = std::max(total, (size_t)4 * b->capacity);
+        if (e == cudaSuccess)
+            e = cudaMalloc(&b->d_steps, 3 * cap * sizeof(double));
+        if (e == cudaSuccess)
+            e = cudaMallocHost(&b->h_steps, 3 * cap * sizeof(double));
+        if (e != cudaSuccess)
+            return cuda_status(e, "vsmc_cuda_cv_batch_read_steps: buffers");
+        b->steps_cap = cap;
+    }
+    e = cudaEventSynchronize(b->staged);
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_cv_batch_read_steps");
+    size_t off = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        ObsRecord r;
+        r.slot = (int32_t)slots[k];
+        r.count = (int32_t)counts[k];
+        r.index = (long long)(b->t[slots[k]] - counts[k]);
+        r.src = (long long)off;
+        b->h_rec[k] = r;
+        off += counts[k];
+    }
+    e = cudaMemcpyAsync(b->d_rec, b->h_rec, n * sizeof(ObsRecord),
+                        cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaEventRecord(b->staged, b->stream);
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_cv_batch_read_steps");
+    kb_read_steps<<<n, 32, 0, b->stream>>>(b->d_slots, b->d_rec, b->d_steps,
+                                           b->d_out);
+    ++b->launches;
+    e = cudaMemcpyAsync(b->h_steps, b->d_steps, 3 * total * sizeof(double),
+                        cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->h_out, b->d_out, n * sizeof(double),
+                            cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_cv_batch_read_steps");
+    int err = VSMC_CUDA_OK;
+    for (size_t i = 0; i < total; ++i) {
+        const double *o = b->h_steps + 3 * i;
+        if (ess)
+            ess[i] = o[0];
+        if (logz_inc)
+            logz_inc[i] = o[1];
+        if (resampled)
+            resampled[i] = (int32_t)o[2];
+    }
+    for (uint32_t k = 0; k < n; ++k) {
+        const int code = (int)b->h_out[k];
+        if (status)
+            status[k] = code;
+        if (code != VSMC_CUDA_OK && err == VSMC_CUDA_OK)
+            err = code;
+    }
+    if (err != VSMC_CUDA_OK)
+        set_last_error("vsmc_cuda_cv_batch_read_steps: a filter's weights "
+                       "are degenerate");
+    return err;
 }
 
 int vsmc_cuda_cv_batch_read_last(vsmc_cuda_cv_batch *b, uint32_t n,

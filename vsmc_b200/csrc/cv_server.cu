@@ -10,10 +10,17 @@
 //   1. release the slots of requests that are closed and fully processed;
 //   2. admit waiting requests in arrival order while a slot and the HBM
 //      budget allow (a request that does not fit waits for memory to free);
-//   3. take the oldest pending observation of every admitted request and
-//      run one step of all of them together (append, step, read back);
+//   3. take up to kCatchUp of the oldest pending observations of every
+//      admitted request and run them together: append them, step every
+//      filter through its own (one launch sequence per step over the
+//      filters still stepping), read the steps back once;
 //   4. publish one result per observation with its arrival and completion
 //      times.
+//
+// A request whose observations arrive faster than ticks complete catches
+// up several steps in one tick instead of one per tick, so the loop's fixed
+// cost per tick (staging, the read-back, the host round trip) is shared by
+// more steps as the load rises.
 //
 // Requests that arrive while a tick runs join the next tick, so their work
 // shares launches with the filters already on the device.  Each filter's
@@ -21,6 +28,7 @@
 // whatever it was batched with.
 #include "../../include/vsmc_cuda.h"
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -57,7 +65,10 @@ struct Request {
     std::deque<PendingObs> pending;
     bool closed = false;
     int32_t status = VSMC_CUDA_OK;
+    double logz = 0.0; // running log-evidence, summed as the device sums it
 };
+
+constexpr uint32_t kCatchUp = 32; // steps per request per tick at most
 
 } // namespace
 
@@ -98,9 +109,9 @@ struct vsmc_cuda_cv_server {
 void vsmc_cuda_cv_server::run()
 {
     cudaSetDevice(device);
-    std::vector<uint32_t> release, tick_slots;
+    std::vector<uint32_t> release, tick_slots, counts, round_slots;
     std::vector<uint64_t> tick_ids, tick_t;
-    std::vector<double> xs, ys, ess, dz, logz;
+    std::vector<double> xs, ys, rx, ry, ess, dz;
     std::vector<int32_t> res, status;
     std::vector<int64_t> sub;
     struct Candidate {
@@ -179,10 +190,12 @@ void vsmc_cuda_cv_server::run()
             }
             got.emplace_back(c.id, slot);
         }
-        // 3. one observation of each admitted request with one pending
+        // 3. up to kCatchUp observations of each admitted request with any
+        // pending, packed request by request
         tick_slots.clear();
         tick_ids.clear();
         tick_t.clear();
+        counts.clear();
         xs.clear();
         ys.clear();
         sub.clear();
@@ -226,14 +239,20 @@ void vsmc_cuda_cv_server::run()
                 Request &r = reqs[id];
                 if (r.pending.empty())
                     continue;
-                const PendingObs o = r.pending.front();
-                r.pending.pop_front();
+                const uint32_t m = (uint32_t)std::min<size_t>(
+                    r.pending.size(), (size_t)kCatchUp);
                 tick_slots.push_back((uint32_t)r.slot);
                 tick_ids.push_back(id);
-                tick_t.push_back(r.stepped++);
-                xs.push_back(o.x);
-                ys.push_back(o.y);
-                sub.push_back(o.submit_ns);
+                tick_t.push_back(r.stepped);
+                counts.push_back(m);
+                for (uint32_t j = 0; j < m; ++j) {
+                    const PendingObs o = r.pending.front();
+                    r.pending.pop_front();
+                    xs.push_back(o.x);
+                    ys.push_back(o.y);
+                    sub.push_back(o.submit_ns);
+                }
+                r.stepped += m;
             }
             if (active.size() > st.max_active)
                 st.max_active = active.size();
@@ -242,20 +261,41 @@ void vsmc_cuda_cv_server::run()
             continue;
         const int64_t begin = now_ns();
         const uint32_t n = (uint32_t)tick_slots.size();
-        ess.assign(n, 0.0);
-        dz.assign(n, 0.0);
-        logz.assign(n, 0.0);
-        res.assign(n, 0);
+        const size_t total = xs.size();
+        uint32_t maxm = 0;
+        for (uint32_t m : counts)
+            maxm = std::max(maxm, m);
+        ess.assign(total, 0.0);
+        dz.assign(total, 0.0);
+        res.assign(total, 0);
         status.assign(n, 0);
-        int rc = vsmc_cuda_cv_batch_append_observations(
-            batch, n, tick_slots.data(), xs.data(), ys.data());
+        // append round j: observation j of every request with more than j
+        int rc = VSMC_CUDA_OK;
+        for (uint32_t j = 0; j < maxm && rc == VSMC_CUDA_OK; ++j) {
+            round_slots.clear();
+            rx.clear();
+            ry.clear();
+            size_t off = 0;
+            for (uint32_t k = 0; k < n; ++k) {
+                if (counts[k] > j) {
+                    round_slots.push_back(tick_slots[k]);
+                    rx.push_back(xs[off + j]);
+                    ry.push_back(ys[off + j]);
+                }
+                off += counts[k];
+            }
+            rc = vsmc_cuda_cv_batch_append_observations(
+                batch, (uint32_t)round_slots.size(), round_slots.data(),
+                rx.data(), ry.data());
+        }
+        // every filter steps through its appended observations
         if (rc == VSMC_CUDA_OK)
-            rc = vsmc_cuda_cv_batch_step(batch, n, tick_slots.data());
+            rc = vsmc_cuda_cv_batch_run(batch, n, tick_slots.data());
         if (rc == VSMC_CUDA_OK || rc == VSMC_CUDA_EDEGENERATE)
-            rc = vsmc_cuda_cv_batch_read_last(batch, n, tick_slots.data(),
-                                              ess.data(), dz.data(),
-                                              res.data(), logz.data(),
-                                              status.data());
+            rc = vsmc_cuda_cv_batch_read_steps(batch, n, tick_slots.data(),
+                                               counts.data(), ess.data(),
+                                               dz.data(), res.data(),
+                                               status.data());
         const int64_t done = now_ns();
         const bool fatal = rc != VSMC_CUDA_OK && rc != VSMC_CUDA_EDEGENERATE;
         uint64_t psteps = 0;
@@ -265,28 +305,41 @@ void vsmc_cuda_cv_server::run()
                 loop_status = rc;
                 loop_error = "tick failed (status " + std::to_string(rc) + ")";
             }
+            size_t off = 0;
             for (uint32_t k = 0; k < n; ++k) {
-                vsmc_cuda_cv_result r;
-                r.request = tick_ids[k];
-                r.t = tick_t[k];
-                r.ess = ess[k];
-                r.logz_inc = dz[k];
-                r.log_evidence = logz[k];
-                r.resampled = res[k];
-                r.status = fatal ? rc : status[k];
-                r.submit_ns = sub[k];
-                r.done_ns = done;
-                results.push_back(r);
                 auto it = reqs.find(tick_ids[k]);
-                if (it != reqs.end()) {
-                    psteps += it->second.N;
-                    if (r.status != VSMC_CUDA_OK)
+                double lz = it != reqs.end() ? it->second.logz : 0.0;
+                for (uint32_t j = 0; j < counts[k]; ++j) {
+                    const size_t i = off + j;
+                    vsmc_cuda_cv_result r;
+                    r.request = tick_ids[k];
+                    r.t = tick_t[k] + j;
+                    r.ess = ess[i];
+                    r.logz_inc = dz[i];
+                    lz = lz + dz[i];
+                    r.log_evidence = lz;
+                    r.resampled = res[i];
+                    // a step's status: the slot's sticky status from the
+                    // step whose ESS it made undefined (the weights turned
+                    // degenerate there), and on the tick's last step
+                    const bool hit = ess[i] != ess[i] || j + 1 == counts[k];
+                    r.status = fatal ? rc
+                                     : (hit ? status[k] : VSMC_CUDA_OK);
+                    r.submit_ns = sub[i];
+                    r.done_ns = done;
+                    results.push_back(r);
+                    if (it != reqs.end() && r.status != VSMC_CUDA_OK)
                         it->second.status = r.status;
                 }
+                if (it != reqs.end()) {
+                    it->second.logz = lz;
+                    psteps += it->second.N * counts[k];
+                }
+                off += counts[k];
             }
-            obs_done += n;
+            obs_done += total;
             ++st.ticks;
-            st.steps += n;
+            st.steps += total;
             st.particle_steps += psteps;
             st.busy_seconds += (double)(done - begin) * 1e-9;
         }
@@ -331,6 +384,8 @@ int vsmc_cuda_cv_server_create(const vsmc_cuda_cv_config *model,
         delete s;
         return rc;
     }
+    // ticks differ in their filters and step counts: direct launches
+    vsmc_cuda_cv_batch_set_graphs(s->batch, 0);
     try {
         s->loop = std::thread([s] { s->run(); });
     } catch (...) {
