@@ -355,22 +355,13 @@ int vsmc_cuda_cv_create(const vsmc_cuda_cv_config *cfg, void *stream,
     f->rep_flags = nullptr;
     // resample engine: Threefry4x64 seeded seed+2 (Seed::get twice)
     f->eng = cv_resample_engine(cfg->seed);
-    int dev = 0, sms = 148, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cfg->form == VSMC_CUDA_MIXED)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per, k_cv_move<float, false>, kThreads, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per, k_cv_move<double, false>, kThreads, 0);
-    if (per < 1)
-        per = 1;
-    const long long g = (long long)sms * per;
     cudaFuncSetAttribute(k_cv_finalize,
                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                          kFinalSmemTiles * (int)sizeof(double));
-    f->move_grid = (int)(f->ntiles < g ? f->ntiles : g);
+    // one CTA per tile: the block scheduler hands tiles to SMs as they
+    // free, which balances the rejection loops' uneven cost better than a
+    // persistent grid striding over tiles (measured 5% faster at 2^24)
+    f->move_grid = (int)f->ntiles;
     e = cudaMemsetAsync(f->mem, 0, f->bytes, f->stream);
     if (e != cudaSuccess) {
         cudaFree(f->mem);
