@@ -391,7 +391,7 @@ int vsmc_cuda_cv_batch_synchronize(vsmc_cuda_cv_batch *b);
 int vsmc_cuda_cv_batch_set_graphs(vsmc_cuda_cv_batch *b, int enable);
 
 /* The launch shape of later steps: the move compiled for `move_blocks`
- * (2, 3 or 4) CTAs per SM, the finalize CTA at `final_threads` (1024 or
+ * (2, 3 or 4) x 256 threads per SM, the finalize CTA at `final_threads` (1024 or
  * 256; 256 applies only while every admitted filter has at most 256 tiles
  * of 2048 particles).  No shape changes a result.  New batches start at
  * (4, 256). */
@@ -400,7 +400,7 @@ int vsmc_cuda_cv_batch_set_launch_shape(vsmc_cuda_cv_batch *b,
 
 /* The batch's autotuner: times a few steps of a trial copy of (a sample
  * of at most 256 of) the listed filters, with zero observations, under each
- * launch shape (the move compiled for 2, 3 or 4 CTAs per SM; the finalize
+ * launch shape (the move compiled for 2, 3 or 4 x 256 threads per SM; the finalize
  * CTA at 1024 or 256 threads when every filter has at most 256 tiles) and
  * keeps the fastest for later steps.  The shapes change no result, and the
  * trial touches none of the batch's filters.  Synchronises; reports the

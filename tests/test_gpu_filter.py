@@ -79,16 +79,27 @@ def test_fp64_large_against_oracle(capi, N, sch):
 
 @pytest.mark.parametrize("sch", [0, 3])
 def test_mixed_form_short_horizon(golden, capi, sch):
-    """Over a few steps the mixed form follows the FP64 ancestry exactly
-    (the polar acceptance is exact, positions are anchored on the
-    observation) and its log-evidence agrees to RTOL_MIXED."""
+    """Free-running over five steps at N = 1000.  Before the first
+    resampling the mixed form is the FP64 step in float: ESS and the
+    evidence increment agree to RTOL_MIXED.  After it, float weights can
+    move a uniform across a cumulative-weight boundary (at N = 1000 a few
+    times in ten steps), so the two ancestries may part: the mixed form
+    must then make the FP64 decision wherever the FP64 ESS is clear of the
+    threshold by 5% of N, and its ESS and log-evidence stay within that
+    Monte Carlo spread.  The precision of the form itself is measured on the
+    FP64 run's ancestry (test_mixed_form_fixed_ancestry)."""
+    N = 1000
     ox, oy = golden["cv_obs_x"][:5], golden["cv_obs_y"][:5]
-    a = run_gpu(capi, 1000, 5, sch, ox, oy)
-    b = run_gpu(capi, 1000, 5, sch, ox, oy, form=capi.MIXED)
-    assert np.array_equal(a["resampled"], b["resampled"])
+    a = run_gpu(capi, N, 5, sch, ox, oy)
+    b = run_gpu(capi, N, 5, sch, ox, oy, form=capi.MIXED)
+    assert abs(a["ess"][0] - b["ess"][0]) <= RTOL_MIXED * a["ess"][0]
+    assert abs(a["logz_inc"][0] - b["logz_inc"][0]) <= RTOL_MIXED * abs(a["logz_inc"][0])
+    clear = np.abs(a["ess"] / N - 0.5) > 0.05
+    assert np.array_equal(a["resampled"][clear], b["resampled"][clear])
+    assert np.all(np.abs(a["ess"] - b["ess"]) <= 0.05 * N)
     err = abs(a["logz"] - b["logz"]) / abs(a["logz"])
     print(f"mixed form, 5 steps, scheme {sch}: rel err {err:.3e}")
-    assert err <= RTOL_MIXED
+    assert err <= 1e-2
 
 
 def replay_pair(capi, N, T, sch, ox, oy):

@@ -111,10 +111,10 @@ static __global__ void kb_expand(const BatchSlot *slots, const int32_t *work,
         map[tile0[w] + k] = TileRef{slot, k};
 }
 
-// MinBlocks: CTAs per SM the move is compiled for (a tuning choice of
+// MinBlocks: 256-thread groups per SM the move is compiled for (a tuning choice of
 // vsmc_cuda_cv_batch_autotune; every variant computes the same values).
 template <typename Real, int MinBlocks>
-__global__ void __launch_bounds__(kThreads, MinBlocks)
+__global__ void __launch_bounds__(kMoveThreads, MinBlocks * 256 / kMoveThreads)
 kb_move(const BatchSlot *slots, const TileRef *map, CVParam p)
 {
     __shared__ double sh_w[7 * kMoveWarps];
@@ -475,7 +475,7 @@ struct vsmc_cuda_cv_batch {
     const TileRef *run_map;
     uint64_t run_launches;
     // launch shapes (vsmc_cuda_cv_batch_autotune); no result depends on them
-    int tune_move;        // CTAs per SM the move is compiled for: 2, 3, 4
+    int tune_move;        // x 256 threads per SM the move is compiled for: 2, 3, 4
     int tune_final;       // finalize CTA size: 256 or 1024
     int max_ntiles;       // largest slot admitted, in tiles
 };
@@ -627,13 +627,13 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
     const int32_t *work = b->d_work;
     switch (b->tune_move) {
     case 2:
-        kb_move<Real, 2><<<nt, kThreads, 0, s>>>(sl, map, b->bc.p);
+        kb_move<Real, 2><<<nt, kMoveThreads, 0, s>>>(sl, map, b->bc.p);
         break;
     case 4:
-        kb_move<Real, 4><<<nt, kThreads, 0, s>>>(sl, map, b->bc.p);
+        kb_move<Real, 4><<<nt, kMoveThreads, 0, s>>>(sl, map, b->bc.p);
         break;
     default:
-        kb_move<Real, 3><<<nt, kThreads, 0, s>>>(sl, map, b->bc.p);
+        kb_move<Real, 3><<<nt, kMoveThreads, 0, s>>>(sl, map, b->bc.p);
         break;
     }
     // a finalize CTA narrower than 1024 threads gives the same sums only

@@ -135,9 +135,9 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
         cudaEventRecord(ev[0], s);
     }
     if (init)
-        k_cv_move<Real, true><<<f->move_grid, kThreads, 0, s>>>(a);
+        k_cv_move<Real, true><<<f->move_grid, kMoveThreads, 0, s>>>(a);
     else
-        k_cv_move<Real, false><<<f->move_grid, kThreads, 0, s>>>(a);
+        k_cv_move<Real, false><<<f->move_grid, kMoveThreads, 0, s>>>(a);
     if (ev)
         cudaEventRecord(ev[1], s);
     f->cur = dst;

@@ -296,7 +296,12 @@ __device__ __forceinline__ MoveStep<Real> move_step(const MoveArgs<Real> &a)
     return m;
 }
 
-constexpr int kMoveWarps = kThreads / 32;
+// A move CTA of 8 warps (8 particles per thread per tile).  4-warp CTAs
+// measured 1.3% faster at 2^24 particles but 20% slower at 2^16, where 32
+// tiles leave most SMs idle and a tile's latency is the step's.
+constexpr int kMoveThreads = 256;                 // threads of a move CTA
+constexpr int kMoveItems = kTile / kMoveThreads; // particles per thread
+constexpr int kMoveWarps = kMoveThreads / 32;
 
 // One tile of kTile particles: load (gather), move, likelihood, log-weight
 // update and the tile's online log-sum-exp statistics.  `sh_w` holds
@@ -308,7 +313,7 @@ __device__ __forceinline__ void cv_move_tile(const MoveArgs<Real> &a,
                                              int tile, double *sh_w)
 {
     constexpr int V = Vec<Real>::n;
-    constexpr int NV = kItems / V;
+    constexpr int NV = kMoveItems / V;
     typedef typename Vec<Real>::type VT;
     constexpr int NW = kMoveWarps;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -324,7 +329,7 @@ __device__ __forceinline__ void cv_move_tile(const MoveArgs<Real> &a,
 #pragma unroll 1
         for (int v = 0; v < NV; ++v) {
             const long long p0 =
-                base + ((long long)v * kThreads + threadIdx.x) * V;
+                base + ((long long)v * kMoveThreads + threadIdx.x) * V;
             Real s[4][V];
             Real lwv[V];
             const bool full = p0 + V <= N;
@@ -458,7 +463,8 @@ __device__ __forceinline__ void cv_move_tile(const MoveArgs<Real> &a,
 }
 
 template <typename Real, bool Init>
-__global__ void __launch_bounds__(kThreads, VSMC_MOVE_MIN_BLOCKS)
+__global__ void __launch_bounds__(kMoveThreads,
+                                  VSMC_MOVE_MIN_BLOCKS * 256 / kMoveThreads)
 k_cv_move(MoveArgs<Real> a)
 {
     // double-buffered warp partials: one barrier per tile
