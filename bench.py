@@ -481,6 +481,7 @@ def main():
     import torch
 
     from vsmc_b200 import capi
+    from vsmc_b200 import replicas
 
     rank, world, local = rank_env()
     torch.cuda.set_device(local)
@@ -497,7 +498,7 @@ def main():
     T = 1 + W + K
     sch = SCHEMES.index(args.scheme)
     form = capi.MIXED if args.form == "mixed" else capi.FP64
-    ox, oy = capi.cv_simulate(T, OBS_SEED, stream_id=rank)
+    ox, oy = capi.cv_simulate(T, OBS_SEED, stream_id=replicas.replica(rank)["stream_id"])
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
 
@@ -507,13 +508,11 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, dist, device="cuda")
 
-    f = capi.CVFilter(N, T, scheme=sch, form=form, seed=101, stream_id=rank, stream=sp)
+    rep = replicas.replica(rank)  # this rank's filter: its own counter stream
+    f = capi.CVFilter(N, T, scheme=sch, form=form, seed=rep["seed"],
+                      stream_id=rep["stream_id"], stream=sp)
     f.set_observations_host(ox, oy)
 
     # ---- device-timed run: inputs resident in HBM -------------------------
@@ -536,7 +535,7 @@ def main():
     f.synchronize()
     hist = f.history()
     logz = f.log_evidence()  # of this run (initialize() keeps the engine)
-    value = world * N * K / (ms / 1e3)
+    value = replicas.job_throughput(world, N, K, ms / 1e3)
     resampled = hist["resampled"][1 + W:]
     n_res = int(resampled.sum())
 
@@ -559,7 +558,8 @@ def main():
     pin_y = torch.from_numpy(oy).pin_memory()
     out = torch.zeros(3, dtype=torch.float64).pin_memory()
     res = torch.zeros(1, dtype=torch.int32).pin_memory()
-    g = capi.CVFilter(N, T, scheme=sch, form=form, seed=101, stream_id=rank, stream=sp)
+    g = capi.CVFilter(N, T, scheme=sch, form=form, seed=rep["seed"],
+                      stream_id=rep["stream_id"], stream=sp)
     px, py = pin_x.data_ptr(), pin_y.data_ptr()
     g.append_observations(px, py, 1)
     g.initialize()
@@ -577,7 +577,7 @@ def main():
     e2e_logz = g.log_evidence()
     g.close()
     f.close()
-    e2e = world * N * K / e2e_s
+    e2e = replicas.job_throughput(world, N, K, e2e_s)
 
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
