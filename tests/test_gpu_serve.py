@@ -181,3 +181,31 @@ def test_server_catch_up(capi, form):
         assert np.array_equal(r["logz_inc"], h["logz_inc"]), k
         assert np.array_equal(r["resampled"], h["resampled"]), k
         assert np.array_equal(r["log_evidence"], np.cumsum(h["logz_inc"])), k
+
+
+def test_server_degenerate_request_in_a_burst(capi):
+    """A NaN observation in the middle of a burst: that request's steps
+    before it succeed, it and every later step report EDEGENERATE, and the
+    request sharing its ticks is unaffected (equal to its filter alone)."""
+    T = 10
+    ox, oy = capi.cv_simulate(T, obs_seed=500, stream_id=0)
+    bx, by = capi.cv_simulate(T, obs_seed=501, stream_id=1)
+    bad_x = ox.copy()
+    bad_x[3] = np.nan
+    with capi.CVServer(4, scheme=0) as srv:
+        a = srv.open(4096, T, 21, 0)
+        b = srv.open(3000, T, 22, 1)
+        for t in range(T):
+            srv.observe([a, b], [bad_x[t], bx[t]], [oy[t], by[t]])
+        srv.close(a)
+        srv.close(b)
+        res = collect(srv, 2 * T)
+    ra = np.sort(res[res["request"] == a], order="t")
+    rb = np.sort(res[res["request"] == b], order="t")
+    assert np.all(ra["status"][:3] == 0)
+    assert np.all(ra["status"][3:] == capi.EDEGENERATE)
+    assert np.all(np.isnan(ra["ess"][3:]))
+    assert np.all(rb["status"] == 0)
+    h = alone(capi, 3000, T, 22, 1, bx, by, 0, 0)
+    assert np.array_equal(rb["ess"], h["ess"])
+    assert np.array_equal(rb["logz_inc"], h["logz_inc"])
