@@ -554,25 +554,38 @@ def main():
     step_achieved = step_bytes / (step_ms / 1e3) / 1e9
 
     # ---- end to end through the C ABI with host buffers -------------------
+    # Streaming use: every step copies its observation from pinned host
+    # memory and reads its ESS, increment and flag back to pinned host
+    # memory.  The host enqueues step t before it waits for step t-1's
+    # result (one step in flight), as a streaming caller would.
     pin_x = torch.from_numpy(ox).pin_memory()
     pin_y = torch.from_numpy(oy).pin_memory()
-    out = torch.zeros(3, dtype=torch.float64).pin_memory()
-    res = torch.zeros(1, dtype=torch.int32).pin_memory()
+    outs = torch.zeros((T, 2), dtype=torch.float64).pin_memory()
+    ress = torch.zeros(T, dtype=torch.int32).pin_memory()
+    done = [torch.cuda.Event() for _ in range(T)]
     g = capi.CVFilter(N, T, scheme=sch, form=form, seed=rep["seed"],
                       stream_id=rep["stream_id"], stream=sp)
     px, py = pin_x.data_ptr(), pin_y.data_ptr()
+
+    def stream_step(t):
+        g.append_observations(px + 8 * t, py + 8 * t, 1)
+        g.iterate(1)
+        g.read_step(t, outs[t].data_ptr(), outs[t].data_ptr() + 8,
+                    ress[t:].data_ptr(), False)
+        done[t].record(stream)
+
     g.append_observations(px, py, 1)
     g.initialize()
     for t in range(1, 1 + W):
-        g.append_observations(px + 8 * t, py + 8 * t, 1)
-        g.iterate(1)
-        g.read_step(t, out.data_ptr(), out.data_ptr() + 8, res.data_ptr(), True)
+        stream_step(t)
+        done[t].synchronize()
     barrier()
     t0 = time.perf_counter()
     for t in range(1 + W, T):
-        g.append_observations(px + 8 * t, py + 8 * t, 1)
-        g.iterate(1)
-        g.read_step(t, out.data_ptr(), out.data_ptr() + 8, res.data_ptr(), True)
+        stream_step(t)
+        if t > 1 + W:
+            done[t - 1].synchronize()  # step t-1's result is on the host
+    done[T - 1].synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_logz = g.log_evidence()
     g.close()
