@@ -174,3 +174,27 @@ def test_iterate_beyond_observations(capi):
         f.initialize()
         with pytest.raises(capi.VsmcCudaError):
             f.iterate(5)
+
+
+@pytest.mark.parametrize("form", [0, 1])
+def test_filter_near_maximum_size(capi, form):
+    """2^28 particles (23 GB of FP64 state, 16x the benchmark), resampling
+    at every step: finite ESS, increments and monitor means, every step
+    resampled, and a second run repeats the first bit for bit."""
+    N, T = 1 << 28, 4
+    ox, oy = capi.cv_simulate(T, 7)
+    runs = []
+    for _ in range(2):
+        with capi.CVFilter(N, T, scheme=0, form=form, threshold=1.1, seed=9) as f:
+            f.set_observations_host(ox, oy)
+            f.initialize()
+            f.iterate(T - 1)
+            h = f.history()
+            h["logz"] = f.log_evidence()
+        runs.append(h)
+    h = runs[0]
+    assert np.all(h["resampled"] == 1)
+    for k in ("ess", "logz_inc", "mean_x", "mean_y"):
+        assert np.all(np.isfinite(h[k])), k
+        assert np.array_equal(h[k], runs[1][k]), k
+    assert np.isfinite(h["logz"]) and h["logz"] == runs[1]["logz"]

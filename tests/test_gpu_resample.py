@@ -139,6 +139,29 @@ def test_sparse_parents_against_oracle(capi, stride, sch):
     assert np.array_equal(cf, ref_cf)
 
 
+@pytest.mark.parametrize("sch", [0, 3, 4])
+def test_invariants_near_maximum_size(capi, sch):
+    """At 2^27 + 5 particles (8x the benchmark; the 32-bit counts and
+    indices of the inversion and cfrp fill at scale): sum rep = N, survivors
+    keep their slot, every copy_from source is a survivor, bincount of
+    copy_from equals rep, the engine advanced, and a second call repeats the
+    first bit for bit."""
+    N = (1 << 27) + 5
+    rng = np.random.default_rng(sch + 40)
+    w = rng.gamma(0.5, size=N)
+    w /= w.sum()
+    a = gpu_resample(capi, sch, w, 17, 0)
+    b = gpu_resample(capi, sch, w, 17, 0)
+    rep, cf, words = a
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+    assert words > 0
+    assert rep.sum() == N and rep.min() >= 0
+    keep = rep > 0
+    assert np.array_equal(cf[keep], np.nonzero(keep)[0])
+    assert np.all(keep[cf])
+    assert np.array_equal(np.bincount(cf, minlength=N), rep)
+
+
 def test_degenerate_and_equal_weights(capi):
     N = 1 << 16
     w = np.zeros(N)
