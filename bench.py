@@ -1,6 +1,6 @@
 #!/usr/bin/env python3
 """SMC step throughput on B200: the constant-velocity Student-t bootstrap
-filter at N = 2^24 particles (BASELINE config 2 shape), one JSON line.
+filter at N = 2^24 particles, Multinomial resampling, FP64, one JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--particles P] [--scheme NAME] [--form fp64|mixed]
