@@ -307,6 +307,11 @@ typedef struct vsmc_cuda_cv_batch vsmc_cuda_cv_batch;
 uint64_t vsmc_cuda_cv_batch_slot_bytes(const vsmc_cuda_cv_config *model,
                                        uint64_t N, uint64_t T_max);
 
+/* A batch of up to `capacity` slots.  hbm_budget > 0 caps the bytes the
+ * admitted slots may hold (admission past it returns VSMC_CUDA_ENOMEM) and
+ * is reserved in the batch's memory pool at creation when the device has
+ * it, so admissions reuse held memory instead of growing the pool; 0 means
+ * no cap and no reservation. */
 int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
                               uint32_t capacity, uint64_t hbm_budget,
                               void *stream, vsmc_cuda_cv_batch **out);

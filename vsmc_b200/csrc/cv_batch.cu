@@ -821,6 +821,19 @@ int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
     // keep freed slots' memory in the pool for the next admissions
     uint64_t keep = ~0ull;
     cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (hbm_budget > 0) {
+        // hold the budget from the start: admissions then carve slots out
+        // of memory the pool already has instead of growing it one slot at
+        // a time (which stalled a busy serving loop); best effort
+        void *r = nullptr;
+        if (cudaMallocFromPoolAsync(&r, hbm_budget, b->pool, b->stream) ==
+            cudaSuccess) {
+            cudaFreeAsync(r, b->stream);
+            cudaStreamSynchronize(b->stream);
+        } else {
+            cudaGetLastError();
+        }
+    }
     const size_t n = capacity;
     e = cudaMalloc(&b->d_slots, n * sizeof(BatchSlot));
     if (e == cudaSuccess)
