@@ -804,6 +804,48 @@ class CVBatch
               "vsmc_cuda_cv_batch_read_last");
         return z;
     }
+    // Appends one observation to each listed slot.
+    void append(const std::vector<std::uint32_t> &slots,
+                const std::vector<double> &x, const std::vector<double> &y)
+    {
+        check(vsmc_cuda_cv_batch_append_observations(
+                  b_, static_cast<std::uint32_t>(slots.size()), slots.data(),
+                  x.data(), y.data()),
+              "vsmc_cuda_cv_batch_append_observations");
+    }
+    // The last counts[k] steps of each slot, packed in list order.
+    struct Steps {
+        std::vector<double> ess, logz_inc;
+        std::vector<std::int32_t> resampled, status;
+    };
+    Steps read_steps(const std::vector<std::uint32_t> &slots,
+                     const std::vector<std::uint32_t> &counts)
+    {
+        std::size_t total = 0;
+        for (std::uint32_t c : counts)
+            total += c;
+        Steps r;
+        r.ess.resize(total);
+        r.logz_inc.resize(total);
+        r.resampled.resize(total);
+        r.status.resize(slots.size());
+        const int st = vsmc_cuda_cv_batch_read_steps(
+            b_, static_cast<std::uint32_t>(slots.size()), slots.data(),
+            counts.data(), r.ess.data(), r.logz_inc.data(),
+            r.resampled.data(), r.status.data());
+        if (st != VSMC_CUDA_EDEGENERATE) // reported per slot in r.status
+            check(st, "vsmc_cuda_cv_batch_read_steps");
+        return r;
+    }
+    // Times the launch shapes on a trial copy of (a sample of) the slots and
+    // keeps the fastest; no result changes.
+    void autotune(const std::vector<std::uint32_t> &slots)
+    {
+        check(vsmc_cuda_cv_batch_autotune(
+                  b_, static_cast<std::uint32_t>(slots.size()), slots.data(),
+                  nullptr, nullptr),
+              "vsmc_cuda_cv_batch_autotune");
+    }
     vsmc_cuda_cv_batch *handle() { return b_; }
 
   private:

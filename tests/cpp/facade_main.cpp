@@ -24,6 +24,7 @@
 //       first column (N doubles) and prints the engine words drawn.
 #include <vsmc_b200/vsmc_cuda.hpp>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -200,6 +201,42 @@ int gmm(int argc, char **argv)
     return 0;
 }
 
+// Many filters through vsmc_b200::CVBatch: autotune, then the series fed
+// three observations per filter at a time (append, run, read_steps).
+// Writes each filter's ESS then its log-evidence increments (n x T each).
+int batch(int argc, char **argv)
+{
+    if (argc != 6)
+        return 2;
+    const std::uint32_t n = static_cast<std::uint32_t>(std::atoi(argv[2]));
+    const std::size_t T = std::strtoull(argv[3], nullptr, 10);
+    std::vector<double> obs = read_bin<double>(argv[4], 2 * T);
+    vsmc_b200::CVBatch b(n, vsmc_b200::Multinomial);
+    std::vector<std::uint32_t> slots(n);
+    for (std::uint32_t k = 0; k != n; ++k)
+        slots[k] = b.admit(1000 + 517 * k, T, 101 + k, k);
+    b.autotune(slots);
+    std::vector<double> ess(n * T), dz(n * T);
+    for (std::size_t t0 = 0; t0 < T; t0 += 3) {
+        const std::size_t m = std::min<std::size_t>(3, T - t0);
+        for (std::size_t j = 0; j != m; ++j)
+            b.append(slots, std::vector<double>(n, obs[t0 + j]),
+                     std::vector<double>(n, obs[T + t0 + j]));
+        b.run(slots);
+        const vsmc_b200::CVBatch::Steps r = b.read_steps(
+            slots, std::vector<std::uint32_t>(n, static_cast<std::uint32_t>(m)));
+        for (std::uint32_t k = 0; k != n; ++k)
+            for (std::size_t j = 0; j != m; ++j) {
+                ess[k * T + t0 + j] = r.ess[k * m + j];
+                dz[k * T + t0 + j] = r.logz_inc[k * m + j];
+            }
+    }
+    std::vector<double> out(ess);
+    out.insert(out.end(), dz.begin(), dz.end());
+    write_bin(argv[5], out);
+    return 0;
+}
+
 } // namespace
 
 int main(int argc, char **argv)
@@ -218,6 +255,8 @@ int main(int argc, char **argv)
             return particle(argc, argv);
         if (cmd == "gmm")
             return gmm(argc, argv);
+        if (cmd == "batch")
+            return batch(argc, argv);
     } catch (const vsmc_b200::RuntimeError &e) {
         std::fprintf(stderr, "RuntimeError %d: %s\n", e.status(), e.what());
         return 3;

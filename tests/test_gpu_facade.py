@@ -136,3 +136,25 @@ def test_gmm_sampler_summary_matches_reference(exe, tmp_path):
         assert out.read_text() == f.read()
     assert abs(smc - float(g["logz"])) <= 1e-9 * abs(float(g["logz"]))
     assert abs(path - float(g["path_logz"])) <= 1e-9 * abs(float(g["path_logz"]))
+
+
+def test_batch_facade_equals_filters_alone(exe, tmp_path):
+    """vsmc_b200::CVBatch (autotune, append, run, read_steps): every filter's
+    ESS and log-evidence increments equal the filter run alone."""
+    from vsmc_b200 import capi as C
+
+    n, T = 5, 14
+    ox, oy = C.cv_simulate(T, obs_seed=77)
+    obs = tmp_path / "obs.bin"
+    np.concatenate([ox, oy]).tofile(obs)
+    out = tmp_path / "out.bin"
+    run(exe, "batch", n, T, obs, out)
+    got = np.fromfile(out, dtype=np.float64).reshape(2, n, T)
+    for k in range(n):
+        with C.CVFilter(1000 + 517 * k, T, seed=101 + k, stream_id=k) as f:
+            f.set_observations_host(ox, oy)
+            f.initialize()
+            f.iterate(T - 1)
+            h = f.history()
+        assert np.array_equal(got[0, k], h["ess"]), k
+        assert np.array_equal(got[1, k], h["logz_inc"]), k
