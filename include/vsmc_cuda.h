@@ -188,7 +188,13 @@ void vsmc_cuda_cv_config_default(vsmc_cuda_cv_config *cfg);
 size_t vsmc_cuda_cv_device_bytes(const vsmc_cuda_cv_config *cfg);
 
 /* Sampler<T>(N, scheme, threshold) (core/sampler.hpp:80-104).  All device
- * memory is allocated here; later calls allocate nothing. */
+ * memory is allocated here; later calls allocate nothing.  A Multinomial
+ * filter also creates a second, internal stream: the sorted U01 sequence of
+ * the next resampling (which depends only on N and the engine position) is
+ * drawn there while the step's move runs; it writes only the filter's own
+ * workspace, and the filter's stream waits for it where it is read.  After
+ * an iterate of more than one step the filter's stream also waits for the
+ * sequence it left running. */
 int vsmc_cuda_cv_create(const vsmc_cuda_cv_config *cfg, void *stream,
                         vsmc_cuda_cv_filter **out);
 int vsmc_cuda_cv_destroy(vsmc_cuda_cv_filter *f);

@@ -60,6 +60,12 @@ struct vsmc_cuda_cv_filter {
     int32_t *rec_cf;            // T_max x N, device, caller-owned
     const int32_t *rep_cf;      // T_max x N, device, caller-owned
     const int32_t *rep_flags;   // T_max, device, caller-owned
+    // Multinomial: the sorted U01 sequence of the next resampling is drawn
+    // on `side` while the step's move and weights run on `stream`
+    cudaStream_t side;
+    cudaEvent_t ev_pos;  // on stream: the engine position is final
+    cudaEvent_t ev_seq;  // on side: the sequence for that position is held
+    bool seq_pending;    // a sequence is enqueued after the last ev_pos
 };
 
 namespace {
@@ -96,6 +102,30 @@ int check_config(const vsmc_cuda_cv_config *c)
     return VSMC_CUDA_OK;
 }
 
+// Multinomial: enqueue the sorted U01 sequence for the engine position the
+// filter's stream has reached, on the side stream (it overlaps the next
+// move and weights; the kernels skip when that position's sequence is held).
+void enqueue_sequence(vsmc_cuda_cv_filter *f)
+{
+    cudaEventRecord(f->ev_pos, f->stream);
+    cudaStreamWaitEvent(f->side, f->ev_pos, 0);
+    launch_spec_sorted((long long)f->cfg.N, f->eng, f->rws, f->side);
+    cudaEventRecord(f->ev_seq, f->side);
+    f->seq_pending = true;
+    f->launches += 4;
+}
+
+// The filter's stream waits for the side stream's last sequence (after a
+// run of several steps, so that the stream's completion covers the work
+// those steps enqueued; single steps leave it running under the next move).
+// The side stream writes only the filter's own workspace, which the next
+// inversion reads after waiting for it.
+void join_sequence(vsmc_cuda_cv_filter *f)
+{
+    if (f->side != nullptr && f->seq_pending)
+        cudaStreamWaitEvent(f->stream, f->ev_seq, 0);
+}
+
 template <typename Real>
 void launch_step(vsmc_cuda_cv_filter *f, bool init)
 {
@@ -121,6 +151,10 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
     a.k1 = 0;
     a.stream = c.stream_id;
     a.p = cv_param(c);
+    // the sequence of this step's resampling, drawn while the move runs
+    const bool speculate = f->side != nullptr && f->rep_cf == nullptr;
+    if (speculate && !f->seq_pending)
+        enqueue_sequence(f);
     cudaEvent_t *ev = nullptr;
     if (f->timing) {
         if (f->ev_used + 3 > f->ev.size()) {
@@ -182,6 +216,13 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
         // recorded decision was to resample)
         cudaMemcpyAsync(f->copy_from, f->rep_cf + (size_t)f->iter * c.N,
                         c.N * 4, cudaMemcpyDeviceToDevice, s);
+    } else if (speculate) {
+        cudaStreamWaitEvent(s, f->ev_seq, 0);
+        launch_resample_core(c.scheme, w, N, f->eng, f->rws, nullptr, 0,
+                             /*spine_done=*/true, nullptr, f->copy_from, s,
+                             /*sorted_ready=*/true);
+        f->launches -= 3; // the sequence's launches are counted on the side
+        enqueue_sequence(f); // for the next resampling
     } else {
         launch_resample_core(c.scheme, w, N, f->eng, f->rws, nullptr, 0,
                              /*spine_done=*/true, nullptr, f->copy_from, s);
@@ -213,6 +254,8 @@ void launch_monitor_flush(vsmc_cuda_cv_filter *f)
 int sync_and_check(vsmc_cuda_cv_filter *f)
 {
     cudaError_t e = cudaStreamSynchronize(f->stream);
+    if (e == cudaSuccess && f->side != nullptr)
+        e = cudaStreamSynchronize(f->side);
     if (e != cudaSuccess)
         return cuda_status(e, "cudaStreamSynchronize");
     FilterCtl h;
@@ -353,6 +396,10 @@ int vsmc_cuda_cv_create(const vsmc_cuda_cv_config *cfg, void *stream,
     f->rec_cf = nullptr;
     f->rep_cf = nullptr;
     f->rep_flags = nullptr;
+    f->side = nullptr;
+    f->ev_pos = nullptr;
+    f->ev_seq = nullptr;
+    f->seq_pending = false;
     // resample engine: Threefry4x64 seeded seed+2 (Seed::get twice)
     f->eng = cv_resample_engine(cfg->seed);
     cudaFuncSetAttribute(k_cv_finalize,
@@ -363,10 +410,27 @@ int vsmc_cuda_cv_create(const vsmc_cuda_cv_config *cfg, void *stream,
     // persistent grid striding over tiles (measured 5% faster at 2^24)
     f->move_grid = (int)f->ntiles;
     e = cudaMemsetAsync(f->mem, 0, f->bytes, f->stream);
+    if (e == cudaSuccess && cfg->scheme == VSMC_CUDA_MULTINOMIAL) {
+        e = cudaStreamCreateWithFlags(&f->side, cudaStreamNonBlocking);
+        if (e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&f->ev_pos, cudaEventDisableTiming);
+        if (e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&f->ev_seq, cudaEventDisableTiming);
+        if (e == cudaSuccess) {
+            k_spec_invalidate<<<1, 1, 0, f->stream>>>(f->rws.ctl);
+            e = cudaGetLastError();
+        }
+    }
     if (e != cudaSuccess) {
+        if (f->side)
+            cudaStreamDestroy(f->side);
+        if (f->ev_pos)
+            cudaEventDestroy(f->ev_pos);
+        if (f->ev_seq)
+            cudaEventDestroy(f->ev_seq);
         cudaFree(f->mem);
         delete f;
-        return cuda_status(e, "vsmc_cuda_cv_create: memset");
+        return cuda_status(e, "vsmc_cuda_cv_create");
     }
     *out = f;
     return VSMC_CUDA_OK;
@@ -377,6 +441,12 @@ int vsmc_cuda_cv_destroy(vsmc_cuda_cv_filter *f)
     if (f == nullptr)
         return VSMC_CUDA_OK;
     cudaStreamSynchronize(f->stream);
+    if (f->side) {
+        cudaStreamSynchronize(f->side);
+        cudaStreamDestroy(f->side);
+        cudaEventDestroy(f->ev_pos);
+        cudaEventDestroy(f->ev_seq);
+    }
     for (cudaEvent_t ev : f->ev)
         cudaEventDestroy(ev);
     cudaError_t e = cudaFree(f->mem);
@@ -448,6 +518,8 @@ int vsmc_cuda_cv_iterate(vsmc_cuda_cv_filter *f, uint64_t num)
         else
             launch_step<double>(f, false);
     }
+    if (num > 1)
+        join_sequence(f);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? VSMC_CUDA_OK
                             : cuda_status(e, "vsmc_cuda_cv_iterate");

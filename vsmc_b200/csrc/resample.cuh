@@ -35,6 +35,8 @@ struct ResampleCtl {
     unsigned long long words;   // engine words drawn by this call
     unsigned long long offset;  // engine offset before the call
     int kbits;            // bin index: K = 2^kbits bins over [0, 1)
+    unsigned long long spec_offset; // engine offset the held speculative
+                                    // sorted sequence was drawn at (~0: none)
 };
 
 struct EngineRef {
@@ -495,16 +497,45 @@ __device__ __forceinline__ void sorted_terms8(const EngineRef &eng,
     }
 }
 
+// Which sorted sequence a launch builds: the step's (ctl->active, NN,
+// kbits), or with spec_N > 0 a speculative Multinomial sequence of spec_N
+// uniforms at the engine's current position, drawn before the step decides
+// to resample (NN = N does not depend on the weights) and skipped when the
+// held sequence was drawn at that position already.
+struct SortedRun {
+    bool run;
+    long long NN;
+    int kbits;
+};
+
+__device__ __forceinline__ SortedRun sorted_run(const ResampleCtl *ctl,
+                                                long long spec_N)
+{
+    SortedRun r;
+    if (spec_N > 0) {
+        r.run = ctl->spec_offset != ctl->offset;
+        r.NN = spec_N;
+        r.kbits = bin_kbits(spec_N);
+    } else {
+        r.run = ctl->active != 0;
+        r.NN = ctl->NN;
+        r.kbits = ctl->kbits;
+    }
+    return r;
+}
+
 // Pass 1: the terms log(1 - U_n) / (NN - n), stored in u[] for pass 2,
 // and their tile sums.
 __device__ __forceinline__ void
 k_sorted_tile_sums_body(EngineRef eng, const ResampleCtl *ctl, double *tile_sum,
-                        double *u, int bid, SmemSortedSums &sm)
+                        double *u, int bid, SmemSortedSums &sm,
+                        long long spec_N = 0)
 {
-    if (!ctl->active)
+    const SortedRun q = sorted_run(ctl, spec_N);
+    if (!q.run)
         return;
     double *sh = sm.sh;
-    const long long NN = ctl->NN;
+    const long long NN = q.NN;
     const long long base = (long long)bid * kTile;
     if (base >= NN)
         return;
@@ -534,12 +565,14 @@ k_sorted_tile_sums(EngineRef eng, const ResampleCtl *ctl, double *tile_sum,
 
 __device__ __forceinline__ void
 k_sorted_spine_body(const double *tile_sum, double *tile_excl,
-                    const ResampleCtl *ctl, int bid, SmemSpine &sm)
+                    const ResampleCtl *ctl, int bid, SmemSpine &sm,
+                    long long spec_N = 0)
 {
-    if (!ctl->active)
+    const SortedRun q = sorted_run(ctl, spec_N);
+    if (!q.run)
         return;
     double *sh = sm.shd;
-    const int ntiles = (int)((ctl->NN + kTile - 1) / kTile);
+    const int ntiles = (int)((q.NN + kTile - 1) / kTile);
     spine_scan_f64(tile_sum, tile_excl, ntiles, 1.0, sh);
 }
 
@@ -554,13 +587,14 @@ k_sorted_spine(const double *tile_sum, double *tile_excl,
 __device__ __forceinline__ void
 k_sorted_uniforms_body(EngineRef eng, const ResampleCtl *ctl,
                        const double *tile_excl, double *u, int32_t *L, int bid,
-                       SmemSortedUniforms &sm)
+                       SmemSortedUniforms &sm, long long spec_N = 0)
 {
-    if (!ctl->active)
+    const SortedRun q = sorted_run(ctl, spec_N);
+    if (!q.run)
         return;
     double *sh = sm.sh;
     double *shm = sm.shm;
-    const long long NN = ctl->NN;
+    const long long NN = q.NN;
     const long long base = (long long)bid * kTile;
     if (base >= NN)
         return;
@@ -610,7 +644,7 @@ k_sorted_uniforms_body(EngineRef eng, const ResampleCtl *ctl,
     for (int w = 0; w < wid; ++w)
         exc = fmax(exc, shm[w]);
     double m = fmax(umax, exc);
-    const int kb = ctl->kbits;
+    const int kb = q.kbits;
     long long kprev = bin_floor(m, kb); // bin of u_{n-1}
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
@@ -631,6 +665,45 @@ k_sorted_uniforms(EngineRef eng, const ResampleCtl *ctl,
 {
     __shared__ SmemSortedUniforms sm;
     k_sorted_uniforms_body(eng, ctl, tile_excl, u, L, blockIdx.x, sm);
+}
+
+// The speculative Multinomial sequence (N uniforms at the engine's current
+// position), on a stream of its own while the step's move and weights run.
+static __global__ void __launch_bounds__(VSMC_SCAN_BOUNDS)
+k_spec_tile_sums(EngineRef eng, const ResampleCtl *ctl, long long N,
+                 double *tile_sum, double *u)
+{
+    __shared__ SmemSortedSums sm;
+    k_sorted_tile_sums_body(eng, ctl, tile_sum, u, blockIdx.x, sm, N);
+}
+
+static __global__ void __launch_bounds__(kSpineThreads)
+k_spec_spine(const double *tile_sum, double *tile_excl,
+             const ResampleCtl *ctl, long long N)
+{
+    __shared__ SmemSpine sm;
+    k_sorted_spine_body(tile_sum, tile_excl, ctl, blockIdx.x, sm, N);
+}
+
+static __global__ void __launch_bounds__(VSMC_SCAN_BOUNDS)
+k_spec_uniforms(EngineRef eng, const ResampleCtl *ctl, long long N,
+                const double *tile_excl, double *u, int32_t *L)
+{
+    __shared__ SmemSortedUniforms sm;
+    k_sorted_uniforms_body(eng, ctl, tile_excl, u, L, blockIdx.x, sm, N);
+}
+
+// The held sequence is now the one for the current position (launched
+// after the three kernels above, which all test the same condition).
+static __global__ void k_spec_commit(ResampleCtl *ctl)
+{
+    ctl->spec_offset = ctl->offset;
+}
+
+// No sequence held (a fresh workspace).
+static __global__ void k_spec_invalidate(ResampleCtl *ctl)
+{
+    ctl->spec_offset = ~0ull;
 }
 
 // ---------------------------------------------------------------------------
@@ -1348,7 +1421,8 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
                                  const EngineRef &eng, ResampleWorkspace &ws,
                                  const double *u_given, long long n_given,
                                  bool spine_done, int32_t *rep_out,
-                                 int32_t *copy_from, cudaStream_t s)
+                                 int32_t *copy_from, cudaStream_t s,
+                                 bool sorted_ready = false)
 {
     const int nt = resample_ntiles(N);
     const bool residual = scheme == VSMC_CUDA_RESIDUAL ||
@@ -1398,7 +1472,7 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
         k_uniforms_stratified<<<(unsigned)((blocks + kThreads - 1) / kThreads),
                                 kThreads, 0, s>>>(eng, ws.ctl, ws.u,
                                                   ws.bins);
-    } else if (!sys) {
+    } else if (!sys && !sorted_ready) {
         k_sorted_tile_sums<<<nt, kThreads, 0, s>>>(eng, ws.ctl,
                                                    ws.u_tile_sum, ws.u);
         k_sorted_spine<<<1, kSpineThreads, 0, s>>>(ws.u_tile_sum,
@@ -1427,6 +1501,21 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
     k_cfrp_fill<<<nt, kThreads, 0, s>>>(N, ws.ctl, ws.sinc, ws.zexcl,
                                         ws.tfirst, ws.tlast, copy_from);
     k_resample_done<<<1, 1, 0, s>>>(ws.ctl);
+}
+
+// The speculative Multinomial sequence for the next resampling (see
+// sorted_run); 4 launches on `s`.
+inline void launch_spec_sorted(long long N, const EngineRef &eng,
+                               ResampleWorkspace &ws, cudaStream_t s)
+{
+    const int nt = resample_ntiles(N);
+    k_spec_tile_sums<<<nt, kThreads, 0, s>>>(eng, ws.ctl, N, ws.u_tile_sum,
+                                             ws.u);
+    k_spec_spine<<<1, kSpineThreads, 0, s>>>(ws.u_tile_sum, ws.u_tile_excl,
+                                             ws.ctl, N);
+    k_spec_uniforms<<<nt, kThreads, 0, s>>>(eng, ws.ctl, N, ws.u_tile_excl,
+                                            ws.u, ws.bins);
+    k_spec_commit<<<1, 1, 0, s>>>(ws.ctl);
 }
 
 } // namespace vsmc_b200
