@@ -454,6 +454,8 @@ def main():
     ap.add_argument("--particles", type=int, default=1 << 24)
     ap.add_argument("--scheme", default="Multinomial", choices=SCHEMES)
     ap.add_argument("--form", default="fp64", choices=("fp64", "mixed"))
+    ap.add_argument("--threshold", type=float, default=0.5,
+                    help="resample when ESS < threshold * N (1.1: every step)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-steps", type=int, default=6)
     ap.add_argument("--no-extras", action="store_true",
@@ -511,7 +513,7 @@ def main():
         return replicas.max_over_ranks(x, dist, device="cuda")
 
     rep = replicas.replica(rank)  # this rank's filter: its own counter stream
-    f = capi.CVFilter(N, T, scheme=sch, form=form, seed=rep["seed"],
+    f = capi.CVFilter(N, T, scheme=sch, form=form, seed=rep["seed"], threshold=args.threshold,
                       stream_id=rep["stream_id"], stream=sp)
     f.set_observations_host(ox, oy)
 
@@ -563,7 +565,7 @@ def main():
     outs = torch.zeros((T, 2), dtype=torch.float64).pin_memory()
     ress = torch.zeros(T, dtype=torch.int32).pin_memory()
     done = [torch.cuda.Event() for _ in range(T)]
-    g = capi.CVFilter(N, T, scheme=sch, form=form, seed=rep["seed"],
+    g = capi.CVFilter(N, T, scheme=sch, form=form, seed=rep["seed"], threshold=args.threshold,
                       stream_id=rep["stream_id"], stream=sp)
     px, py = pin_x.data_ptr(), pin_y.data_ptr()
 
@@ -651,7 +653,7 @@ def main():
             "dtype": "f64" if args.form == "fp64" else "f32+f64",
             "data": "synthetic (simulated CV Student-t series, Philox4x32-10 seed 7)",
             "config": {"workload": f"cv_student_t N={N} T={T} {args.scheme} {args.form} "
-                                   f"threshold 0.5 seed 101",
+                                   f"threshold {args.threshold} seed 101",
                        "particles": N, "scheme": args.scheme, "form": args.form,
                        "resampled_steps": n_res,
                        "l2": "inputs larger than L2 (state 512 MiB FP64 / 256 MiB mixed)",
