@@ -634,7 +634,8 @@ def main():
             "mixed": [serving_point(capi, capi.MIXED, lam, 11) for lam in rates]}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    # the host reference runs the filter at threshold 0.5
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.threshold == 0.5:
         try:
             S = args.cpu_sample_steps
             v, info = cpu_reference(N, sch, 0, 0, sample_steps=S)
