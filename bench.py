@@ -127,26 +127,42 @@ def rank_env():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
-def cpu_reference(N, scheme, warmup, steps, sample_steps=None):
-    """The vSMC reference (oracle/_ref harness, StateOMP, all host threads) on
-    the same filter.  Returns (particle-steps/s over the timed steps, info)."""
+def cpu_reference(N, scheme, warmup, steps, sample_steps=None, backend=0,
+                  threshold=0.5):
+    """The vSMC reference (oracle/_ref harness; backend 0 StateOMP, 1
+    StateSTD; all host threads) on the same filter.  Returns (particle-steps/s
+    over the timed steps, info)."""
     from oracle import oracle as O
 
     T = 1 + warmup + steps if sample_steps is None else 1 + sample_steps
+    first = 1 + (warmup if sample_steps is None else 0)
     ox, oy = O.cv_simulate(T, obs_seed=OBS_SEED)
+    resampled = None
     if O.ref_available():
-        r = O.ref_cv_filter(N, T, scheme, ox, oy, seed=101, backend=0)
-        timed = r["step_seconds"][1 + (warmup if sample_steps is None else 0):]
-        kind, cores = "reference", O.ref_max_threads()
+        r = O.ref_cv_filter(N, T, scheme, ox, oy, seed=101, backend=backend,
+                            threshold=threshold)
+        timed = r["step_seconds"][first:]
+        resampled = int(r["resampled"][first:].sum())
+        kind, cores = "reference", (O.ref_max_threads() if backend == 0
+                                    else os.cpu_count())
     else:
         t0 = time.perf_counter()
-        O.cv_filter(N, T, scheme, ox, oy, seed=101)
+        O.cv_filter(N, T, scheme, ox, oy, seed=101, threshold=threshold)
         timed = [time.perf_counter() - t0]
         kind, cores = "port", 1
-        T = T
     n_steps = len(timed) if kind == "reference" else T
     return N * n_steps / float(sum(timed)), {"kind": kind, "cores": cores,
-                                             "steps": n_steps}
+                                             "steps": n_steps, "resampled": resampled}
+
+
+def workload_config(N, T, scheme, form, threshold, world, resampled):
+    """The `config` object both arms print for the same workload."""
+    return {"workload": f"cv_student_t N={N} T={T} {scheme} {form} "
+                        f"threshold {threshold} seed 101",
+            "particles": N, "scheme": scheme, "form": form,
+            "resampled_steps": resampled,
+            "l2": "inputs larger than L2 (state 512 MiB FP64 / 256 MiB mixed)",
+            "parallelism": "replicas" if world > 1 else "single"}
 
 
 def forms_compare(capi, N, sch, K, W, ox, oy, sp, fp64_step_ms):
@@ -425,22 +441,33 @@ def run_reference_arm(args):
         return 0
     N = args.particles
     sch = SCHEMES.index(args.scheme)
-    v, info = cpu_reference(N, sch, args.warmup, args.steps)
+    T = 1 + args.warmup + args.steps
+    v, info = cpu_reference(N, sch, args.warmup, args.steps, threshold=args.threshold)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * N / v, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"cv_student_t N={N} {args.scheme} fp64 "
-                               f"threshold 0.5 (vSMC Sampler, StateOMP)",
-                   "particles": N, "scheme": args.scheme},
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (simulated CV Student-t series, Philox4x32-10 seed 7)",
+        "config": workload_config(N, T, args.scheme, "fp64", args.threshold, 1,
+                                  info["resampled"]),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"],
                          "kind": info["kind"],
-                         "sample": f"initialize + {args.warmup} warm-up + "
+                         "sample": f"vSMC Sampler with StateOMP/MoveOMP/MonitorEvalOMP: "
+                                   f"initialize + {args.warmup} warm-up + "
                                    f"{args.steps} timed steps at N={N}"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if not args.no_state_std:
+        # vSMC's std::thread backend on a bounded sample of the same filter
+        S = args.cpu_sample_steps
+        vs, infs = cpu_reference(N, sch, 0, 0, sample_steps=S, backend=1,
+                                 threshold=args.threshold)
+        line["state_std"] = {"value": vs, "unit": UNIT, "cores": infs["cores"],
+                             "kind": infs["kind"],
+                             "sample": f"vSMC StateSTD/MoveSTD (std::thread): initialize "
+                                       f"+ {S} steps at N={N}; rate over the {S} steps"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -457,6 +484,8 @@ def main():
     ap.add_argument("--threshold", type=float, default=0.5,
                     help="resample when ESS < threshold * N (1.1: every step)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-state-std", action="store_true",
+                    help="skip the StateSTD (std::thread) host baseline")
     ap.add_argument("--cpu-sample-steps", type=int, default=6)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the form comparison, batched and serving sections")
@@ -530,6 +559,7 @@ def main():
     with torch.cuda.stream(stream):
         e0.record(stream)
         f.iterate(K)
+        f.complete_monitor()  # the last step's monitor, inside the clock
         e1.record(stream)
     barrier()
     clk = clocks.stop()
@@ -642,6 +672,12 @@ def main():
             cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
                    "sample": f"vSMC StateOMP, initialize + {S} steps of the same filter "
                              f"at N={N}; rate over the {S} iterate(1) steps"}
+            if not args.no_state_std:
+                vs, infs = cpu_reference(N, sch, 0, 0, sample_steps=S, backend=1)
+                cpu["state_std"] = {
+                    "value": vs, "unit": UNIT, "cores": infs["cores"], "kind": infs["kind"],
+                    "sample": f"vSMC StateSTD (std::thread), initialize + {S} steps at "
+                              f"N={N}"}
         except Exception as ex:  # reported, never silently replaced
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None,
                    "sample": f"failed: {ex}"}
@@ -653,12 +689,8 @@ def main():
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.form == "fp64" else "f32+f64",
             "data": "synthetic (simulated CV Student-t series, Philox4x32-10 seed 7)",
-            "config": {"workload": f"cv_student_t N={N} T={T} {args.scheme} {args.form} "
-                                   f"threshold {args.threshold} seed 101",
-                       "particles": N, "scheme": args.scheme, "form": args.form,
-                       "resampled_steps": n_res,
-                       "l2": "inputs larger than L2 (state 512 MiB FP64 / 256 MiB mixed)",
-                       "parallelism": "replicas" if world > 1 else "single"},
+            "config": workload_config(N, T, args.scheme, args.form, args.threshold, world,
+                                      n_res),
             "roofline": {"bound": "hbm", "kernel": "k_cv_move",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,

@@ -143,10 +143,12 @@ int vsmc_cuda_resample(int scheme, uint64_t N, const double *weight,
  * particles (about 4.1 MiB on every device that loads the library, kept
  * until exit).  Larger N returns VSMC_CUDA_EINVAL.  It calls no cudaMalloc
  * or cudaFree.  The first call on each device looks up the array's device
- * address (cudaGetSymbolAddress, with that device current) and caches it;
- * make that first call before any stream capture.  All calls share the
- * array: calls that overlap on the GPU race and must be serialised by the
- * caller. */
+ * address (cudaGetSymbolAddress, with that device current) and caches it
+ * with the device's current context (a context created anew, e.g. after
+ * cudaDeviceReset, is looked up again); make that first call before any
+ * stream capture.  Every call waits for `stream` before it returns (it reads
+ * the engine position back).  All calls share the array: calls that overlap
+ * on the GPU race and must be serialised by the caller. */
 int vsmc_cuda_resample_noalloc(int scheme, uint64_t N, const double *weight,
                                const double *uniforms, uint64_t n_uniforms,
                                vsmc_cuda_threefry_state *rng,
@@ -230,6 +232,13 @@ int vsmc_cuda_cv_history(vsmc_cuda_cv_filter *f, double *ess,
                          int32_t *resampled, double *logz_inc, double *mean_x,
                          double *mean_y);
 
+/* Monitor::eval of the last step (core/sampler.hpp:825-834) when that step
+ * resampled: its posterior mean is taken over the gathered parents, which
+ * the next move gathers anyway, so iterate leaves it to that move or to
+ * this call (vsmc_cuda_cv_history makes it too).  Asynchronous; enqueues two
+ * kernels that return at once when there is nothing to complete. */
+int vsmc_cuda_cv_complete_monitor(vsmc_cuda_cv_filter *f);
+
 /* Running log-evidence sum (host scalar).  Synchronises. */
 int vsmc_cuda_cv_log_evidence(vsmc_cuda_cv_filter *f, double *logz);
 
@@ -260,8 +269,13 @@ int vsmc_cuda_cv_read_step(vsmc_cuda_cv_filter *f, uint64_t t, double *ess,
  * and `replay_resampled` (device, T_max int32) the filter skips its own
  * resampling: step t resamples iff replay_resampled[t] != 0 and then takes
  * row t as copy_from, so a run in another precision form follows exactly
- * the recorded ancestry.  Pass NULLs to turn either off.  The arrays stay
- * owned by the caller and must outlive the steps that use them. */
+ * the recorded ancestry.  With all three, the filter follows `replay` and
+ * still resamples on each step's own decision, writing its own copy_from
+ * into row t of `record` (the engine advances by the words it draws): the
+ * step-by-step comparison of the device's resampling with another run's
+ * (the reference's) on a shared trajectory.  Pass NULLs to turn either off.
+ * The arrays stay owned by the caller and must outlive the steps that use
+ * them. */
 int vsmc_cuda_cv_set_ancestry(vsmc_cuda_cv_filter *f, int32_t *record,
                               const int32_t *replay,
                               const int32_t *replay_resampled);

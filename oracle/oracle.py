@@ -41,8 +41,12 @@ _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 
 
 def build() -> None:
-    """Build both checkers (the reference one only where vSMC is present)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    """Build both checkers (the reference one only where the environment's
+    VSMC_ROOT names a vSMC tree; otherwise a prebuilt _ref/ is used)."""
+    cmd = ["make", "-s", "-C", HERE]
+    if os.environ.get("VSMC_ROOT"):
+        cmd.append("VSMC_ROOT=" + os.environ["VSMC_ROOT"])
+    subprocess.run(cmd, check=True)
 
 
 class _CVParam(C.Structure):
@@ -337,6 +341,44 @@ def ref_cv_filter(N, T, scheme, obs_x, obs_y, seed=101, stream=0, threshold=0.5,
     if want_state:
         r["state"] = st.reshape(4, N)
         r["lw"] = lw
+    return r
+
+
+def ref_cv_filter_trace(N, T, scheme, obs_x, obs_y, seed=101, stream=0, threshold=0.5,
+                        param=CV_DEFAULT, nthreads=0, weights_step=None):
+    """vSMC's Sampler (StateOMP) on the filter, with a trace of the run:
+    ``copy_from`` (T x N int32; rows of steps that resampled are
+    Particle::resample's copy_from), ``words_before`` (the resample engine's
+    words drawn before each step's resampling) and, for ``weights_step``, the
+    normalised weights that step resampled with."""
+    ox = np.ascontiguousarray(obs_x, np.float64)
+    oy = np.ascontiguousarray(obs_y, np.float64)
+    L = ref()
+    L.ref_cv_filter_trace.restype = C.c_double
+    L.ref_cv_filter_trace.argtypes = [C.c_int, C.c_void_p, C.c_uint64, C.c_uint64,
+                                      C.c_int, C.c_double, C.c_uint, C.c_uint,
+                                      C.c_void_p, C.c_void_p] + [C.c_void_p] * 8 + [
+                                      C.c_uint64, C.c_void_p, C.c_void_p]
+    r = CVResult(
+        ess=np.zeros(T), resampled=np.zeros(T, np.int32), logz_inc=np.zeros(T),
+        mean_x=np.zeros(T), mean_y=np.zeros(T))
+    r["copy_from"] = np.full((T, N), -1, np.int32)
+    r["words_before"] = np.zeros(T, np.uint64)
+    wu = np.zeros(1, np.uint64)
+    sec = np.zeros(1)
+    w = np.zeros(N) if weights_step is not None else None
+    p = np.asarray(param, np.float64)
+    r["logz"] = L.ref_cv_filter_trace(
+        nthreads, p.ctypes.data, N, T, scheme, threshold, seed, stream,
+        ox.ctypes.data, oy.ctypes.data, r["ess"].ctypes.data, r["resampled"].ctypes.data,
+        r["logz_inc"].ctypes.data, r["mean_x"].ctypes.data, r["mean_y"].ctypes.data,
+        wu.ctypes.data, r["copy_from"].ctypes.data,
+        None if w is None else w.ctypes.data, 0 if weights_step is None else weights_step,
+        r["words_before"].ctypes.data, sec.ctypes.data)
+    r["words_used"] = int(wu[0])
+    r["seconds"] = float(sec[0])
+    if w is not None:
+        r["weights"] = w
     return r
 
 

@@ -53,7 +53,23 @@ class cv_state : public StateB<vsmc::StateMatrix<vsmc::ColMajor, 5, double> >
     typedef StateB<vsmc::StateMatrix<vsmc::ColMajor, 5, double> > base;
     typedef typename base::size_type size_type;
 
-    cv_state (size_type N) : base(N), zconst(0), stream(0) {}
+    cv_state (size_type N) : base(N), zconst(0), stream(0),
+        rec_cf(VSMC_NULLPTR), rec_w(VSMC_NULLPTR), rec_w_step(0),
+        words_before(VSMC_NULLPTR) {}
+
+    // Particle::resample hands the value its copy_from vector here
+    // (core/particle.hpp:245); the trace keeps each step's row before the
+    // backend's own copy runs.
+    template <typename IntType>
+    void copy (size_type N, const IntType *copy_from)
+    {
+        if (rec_cf != VSMC_NULLPTR && copy_from != VSMC_NULLPTR) {
+            const std::size_t row = zinc.size() - 1;
+            for (size_type i = 0; i != N; ++i)
+                rec_cf[row * N + i] = static_cast<int32_t>(copy_from[i]);
+        }
+        base::copy(N, copy_from);
+    }
 
     double log_likelihood (std::size_t iter, size_type id) const
     {
@@ -73,7 +89,30 @@ class cv_state : public StateB<vsmc::StateMatrix<vsmc::ColMajor, 5, double> >
     double zconst;
     std::vector<double> zinc;
     unsigned stream;
+
+    // trace of a run (ref_cv_filter_trace): each step's copy_from (T x N),
+    // the normalised weights one step resamples with, and the resample
+    // engine's word count before each step's resampling
+    int32_t *rec_cf;
+    double *rec_w;
+    std::size_t rec_w_step;
+    uint64_t *words_before;
 };
+
+// Words drawn from a Threefry4x64 engine since its counter was zero.  The
+// buffer index is private, so it is read back from the engine's stream form
+// "ctr(4) par(5) buffer(4) index" (threefry.hpp:425-440).
+uint64_t threefry_words_used (const vsmc::Threefry4x64 &eng)
+{
+    std::stringstream ss;
+    ss << eng;
+    uint64_t v[13];
+    for (int k = 0; k != 13; ++k)
+        ss >> v[k];
+    std::size_t index = 0;
+    ss >> index;
+    return v[0] == 0 ? 0 : (v[0] - 1) * 4 + index;
+}
 
 // Per-particle engine: a copy of the particle's RngSet engine with the
 // counter set to {0, step, id, stream} (pf_smp.hpp:159-164, 218-227).
@@ -111,6 +150,12 @@ void add_with_evidence (vsmc::Particle<T> &particle, std::vector<double> &w,
         particle.weight_set().set_log_weight(&inc[0]);
     else
         particle.weight_set().add_log_weight(&inc[0]);
+    T &value = particle.value();
+    const std::size_t step = value.zinc.size() - 1;
+    if (value.words_before != VSMC_NULLPTR)
+        value.words_before[step] = threefry_words_used(particle.resample_rng());
+    if (value.rec_w != VSMC_NULLPTR && step == value.rec_w_step)
+        particle.weight_set().read_weight(value.rec_w);
 }
 
 template <template <typename> class StateB,
@@ -187,21 +232,6 @@ void cv_est (std::size_t, std::size_t, vsmc::ConstSingleParticle<T> csp,
     res[1] = csp.state(vsmc::Position<1>());
 }
 
-// Words drawn from a Threefry4x64 engine since its counter was zero.  The
-// buffer index is private, so it is read back from the engine's stream form
-// "ctr(4) par(5) buffer(4) index" (threefry.hpp:425-440).
-uint64_t threefry_words_used (const vsmc::Threefry4x64 &eng)
-{
-    std::stringstream ss;
-    ss << eng;
-    uint64_t v[13];
-    for (int k = 0; k != 13; ++k)
-        ss >> v[k];
-    std::size_t index = 0;
-    ss >> index;
-    return v[0] == 0 ? 0 : (v[0] - 1) * 4 + index;
-}
-
 struct run_out {
     double *ess;
     int32_t *resampled;
@@ -214,6 +244,10 @@ struct run_out {
     double *seconds;
     double *step_seconds;
     std::string *summary; // Sampler::print output (sampler.hpp:684-721)
+    int32_t *rec_cf;      // trace: T x N copy_from rows (nullable)
+    double *rec_w;        // trace: the weights step rec_w_step resamples
+    uint64_t rec_w_step;
+    uint64_t *words_before; // trace: T engine word counts (nullable)
 };
 
 template <template <typename> class StateB,
@@ -232,6 +266,12 @@ double run_filter (const cv_param &prm, std::size_t N, std::size_t T,
     sampler.particle().value().obs_x = ox;
     sampler.particle().value().obs_y = oy;
     sampler.particle().value().stream = stream;
+    if (out) {
+        sampler.particle().value().rec_cf = out->rec_cf;
+        sampler.particle().value().rec_w = out->rec_w;
+        sampler.particle().value().rec_w_step = out->rec_w_step;
+        sampler.particle().value().words_before = out->words_before;
+    }
     sampler
         .init(cv_init<StateB, InitB>())
         .move(cv_move<StateB, MoveB>(), false)
@@ -406,7 +446,8 @@ double ref_cv_filter (int backend, int nthreads, const double *param,
     cv_param prm = {param[0], param[1], param[2], param[3], param[4],
         param[5], param[6]};
     run_out out = {ess, resampled, logz_inc, mean_x, mean_y, final_state,
-        final_lw, words_used, seconds, step_seconds, VSMC_NULLPTR};
+        final_lw, words_used, seconds, step_seconds, VSMC_NULLPTR,
+        VSMC_NULLPTR, VSMC_NULLPTR, 0, VSMC_NULLPTR};
     if (nthreads > 0)
         omp_set_num_threads(nthreads);
     switch (backend) {
@@ -437,7 +478,7 @@ uint64_t ref_cv_summary (const double *param, uint64_t N, uint64_t T,
     std::string text;
     run_out out = {VSMC_NULLPTR, VSMC_NULLPTR, VSMC_NULLPTR, VSMC_NULLPTR,
         VSMC_NULLPTR, VSMC_NULLPTR, VSMC_NULLPTR, VSMC_NULLPTR, VSMC_NULLPTR,
-        VSMC_NULLPTR, &text};
+        VSMC_NULLPTR, &text, VSMC_NULLPTR, VSMC_NULLPTR, 0, VSMC_NULLPTR};
     run_filter<vsmc::StateSEQ, vsmc::InitializeSEQ, vsmc::MoveSEQ,
         vsmc::MonitorEvalSEQ>(prm, N, T, scheme, threshold, seed, stream, ox,
                 oy, &out);
@@ -447,6 +488,31 @@ uint64_t ref_cv_summary (const double *param, uint64_t N, uint64_t T,
         buf[n] = '\0';
     }
     return text.size();
+}
+
+// ref_cv_filter (OMP backend) plus a trace of the run: cf (T x N int32,
+// nullable) receives each resampling step's copy_from row as
+// Particle::resample hands it to the value (rows of steps that do not
+// resample are left as they are); w (N doubles, nullable) the normalised
+// weights step w_step resamples with; words_before (T, nullable) the resample
+// engine's words drawn before each step's resampling.
+double ref_cv_filter_trace (int nthreads, const double *param, uint64_t N,
+        uint64_t T, int scheme, double threshold, unsigned seed,
+        unsigned stream, const double *ox, const double *oy, double *ess,
+        int32_t *resampled, double *logz_inc, double *mean_x, double *mean_y,
+        uint64_t *words_used, int32_t *cf, double *w, uint64_t w_step,
+        uint64_t *words_before, double *seconds)
+{
+    cv_param prm = {param[0], param[1], param[2], param[3], param[4],
+        param[5], param[6]};
+    run_out out = {ess, resampled, logz_inc, mean_x, mean_y, VSMC_NULLPTR,
+        VSMC_NULLPTR, words_used, seconds, VSMC_NULLPTR, VSMC_NULLPTR, cf, w,
+        w_step, words_before};
+    if (nthreads > 0)
+        omp_set_num_threads(nthreads);
+    return run_filter<vsmc::StateOMP, vsmc::InitializeOMP, vsmc::MoveOMP,
+           vsmc::MonitorEvalOMP>(prm, N, T, scheme, threshold, seed, stream,
+                   ox, oy, &out);
 }
 
 int ref_max_threads (void) {return omp_get_max_threads();}

@@ -34,6 +34,15 @@ def test_reference_arm_line():
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"],
                            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert line["config"]["particles"] == 65536
+    # the device arm prints the same config object for the same workload
+    sys.path.insert(0, ROOT)
+    import bench
+
+    assert line["config"] == bench.workload_config(
+        65536, 7, "Multinomial", "fp64", 0.5, 1, line["config"]["resampled_steps"])
+    assert line["config"]["workload"] == ("cv_student_t N=65536 T=7 Multinomial fp64 "
+                                          "threshold 0.5 seed 101")
+    assert line["state_std"]["kind"] == "reference" and line["state_std"]["value"] > 0
 
 
 def test_bench_rejects_short_warmup():

@@ -110,6 +110,7 @@ def lib():
     L.vsmc_cuda_cv_read_step.argtypes = [vp, u64, vp, vp, vp, i32]
     L.vsmc_cuda_cv_set_timing.argtypes = [vp, i32]
     L.vsmc_cuda_cv_set_ancestry.argtypes = [vp, vp, vp, vp]
+    L.vsmc_cuda_cv_complete_monitor.argtypes = [vp]
     L.vsmc_cuda_cv_timing.argtypes = [vp, C.POINTER(f64), C.POINTER(f64), C.POINTER(u64),
                                       C.POINTER(u64)]
     L.vsmc_cuda_cv_simulate.argtypes = [C.POINTER(CVConfig), C.c_uint32, u64, vp, vp, vp]
@@ -368,6 +369,10 @@ class CVFilter:
         check(lib().vsmc_cuda_cv_read_step(self.h, t, ess_ptr, logz_ptr, res_ptr,
                                            1 if synchronize else 0),
               "vsmc_cuda_cv_read_step")
+
+    def complete_monitor(self):
+        """Asynchronously completes the last step's monitor (see the C ABI)."""
+        check(lib().vsmc_cuda_cv_complete_monitor(self.h), "vsmc_cuda_cv_complete_monitor")
 
     def set_ancestry(self, record_ptr=None, replay_ptr=None, replay_flags_ptr=None):
         check(lib().vsmc_cuda_cv_set_ancestry(self.h, record_ptr, replay_ptr,

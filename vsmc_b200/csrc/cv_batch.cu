@@ -160,6 +160,7 @@ kb_finalize(const BatchSlot *slots, const int32_t *work, BatchConst c)
     a.sys = c.sys;
     a.eng = b.eng;
     a.replay_flags = nullptr;
+    a.compare = 0;
     k_cv_finalize_body(a, agg, kBatchAgg, sm);
 }
 

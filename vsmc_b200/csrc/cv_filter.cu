@@ -203,6 +203,8 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
     fa.sys = sys;
     fa.eng = f->eng;
     fa.replay_flags = f->rep_flags;
+    const bool compare = f->rep_cf != nullptr && f->rec_cf != nullptr;
+    fa.compare = compare ? 1 : 0;
     const size_t fin_smem = f->ntiles <= kFinalSmemTiles
                                 ? (size_t)f->ntiles * sizeof(double)
                                 : 0;
@@ -212,6 +214,14 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
     w.lw = static_cast<const Real *>(f->lw);
     w.stats = &f->ctl->lw_max;
     if (f->rep_cf != nullptr) {
+        if (compare) {
+            // the step's own resampling of its own weights, into the
+            // record row; the engine advances by the words it drew
+            launch_resample_core(c.scheme, w, N, f->eng, f->rws, nullptr, 0,
+                                 /*spine_done=*/true, nullptr,
+                                 f->rec_cf + (size_t)f->iter * c.N, s);
+            f->launches += resample_launches(c.scheme, false);
+        }
         // replay: the recorded ancestry of this step (used only if the
         // recorded decision was to resample)
         cudaMemcpyAsync(f->copy_from, f->rep_cf + (size_t)f->iter * c.N,
@@ -227,7 +237,7 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
         launch_resample_core(c.scheme, w, N, f->eng, f->rws, nullptr, 0,
                              /*spine_done=*/true, nullptr, f->copy_from, s);
     }
-    if (f->rec_cf != nullptr)
+    if (f->rec_cf != nullptr && !compare)
         cudaMemcpyAsync(f->rec_cf + (size_t)f->iter * c.N, f->copy_from,
                         c.N * 4, cudaMemcpyDeviceToDevice, s);
     if (ev)
@@ -240,13 +250,14 @@ template <typename Real>
 void launch_monitor_flush(vsmc_cuda_cv_filter *f)
 {
     const long long N = (long long)f->cfg.N;
+    const long long t = (long long)f->iter - 1;
     k_cv_monitor_gather<Real><<<kMonParts, kThreads, 0, f->stream>>>(
         static_cast<const Real *>(f->state[f->cur][0]),
         static_cast<const Real *>(f->state[f->cur][1]), f->copy_from, N,
-        f->mon_part);
+        f->mon_part, f->ctl, t);
     const bool anch = f->cfg.form == VSMC_CUDA_MIXED;
     k_cv_monitor_finish<<<1, 32, 0, f->stream>>>(
-        f->mon_part, kMonParts, N, (long long)f->iter - 1, f->ctl,
+        f->mon_part, kMonParts, N, t, f->ctl,
         anch ? f->obs_x : nullptr, anch ? f->obs_y : nullptr,
         f->hist_mean_x, f->hist_mean_y);
 }
@@ -279,25 +290,19 @@ int sync_and_check(vsmc_cuda_cv_filter *f)
     return VSMC_CUDA_OK;
 }
 
-// Gathered monitor of a final resampled step, if not yet written.
+// Gathered monitor of a final resampled step, if not yet written; the
+// kernels read the decision on the device, so nothing waits here.
 int flush_monitor(vsmc_cuda_cv_filter *f)
 {
     if (f->iter == 0)
         return VSMC_CUDA_OK;
-    FilterCtl h;
-    cudaError_t e = cudaMemcpyAsync(&h, f->ctl, sizeof(h),
-                                    cudaMemcpyDeviceToHost, f->stream);
-    if (e == cudaSuccess)
-        e = cudaStreamSynchronize(f->stream);
-    if (e != cudaSuccess)
-        return cuda_status(e, "monitor flush");
-    if (h.resampled && h.monitor_done != (long long)f->iter - 1) {
-        if (f->cfg.form == VSMC_CUDA_MIXED)
-            launch_monitor_flush<float>(f);
-        else
-            launch_monitor_flush<double>(f);
-    }
-    return VSMC_CUDA_OK;
+    if (f->cfg.form == VSMC_CUDA_MIXED)
+        launch_monitor_flush<float>(f);
+    else
+        launch_monitor_flush<double>(f);
+    f->launches += 2;
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VSMC_CUDA_OK : cuda_status(e, "monitor flush");
 }
 
 } // namespace
@@ -540,6 +545,13 @@ int vsmc_cuda_cv_iter_size(vsmc_cuda_cv_filter *f, uint64_t *n)
     return VSMC_CUDA_OK;
 }
 
+int vsmc_cuda_cv_complete_monitor(vsmc_cuda_cv_filter *f)
+{
+    if (f == nullptr)
+        return VSMC_CUDA_EINVAL;
+    return flush_monitor(f);
+}
+
 int vsmc_cuda_cv_history(vsmc_cuda_cv_filter *f, double *ess,
                          int32_t *resampled, double *logz_inc, double *mean_x,
                          double *mean_y)
@@ -723,6 +735,15 @@ int vsmc_cuda_cv_set_ancestry(vsmc_cuda_cv_filter *f, int32_t *record,
         set_last_error("vsmc_cuda_cv_set_ancestry: replay needs both the "
                        "ancestry and the decisions");
         return VSMC_CUDA_EINVAL;
+    }
+    if (f->side != nullptr) {
+        // a speculative sequence still running on the side stream must not
+        // overlap the non-speculative resampling of a replayed step, and the
+        // held one is dropped
+        join_sequence(f);
+        f->seq_pending = false;
+        k_spec_invalidate<<<1, 1, 0, f->stream>>>(f->rws.ctl);
+        ++f->launches;
     }
     f->rec_cf = record;
     f->rep_cf = replay;

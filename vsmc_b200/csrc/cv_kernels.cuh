@@ -499,6 +499,7 @@ struct FinalizeArgs {
     int sys;
     EngineRef eng;
     const int32_t *replay_flags; // replay: resampling decisions to follow
+    int compare; // replay, and still resample on this step's own decision
 };
 
 constexpr int kFinalThreads = 1024;
@@ -648,6 +649,10 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
         } else {
             res = ess < a.threshold * Nd;
         }
+        // the step's own decision runs the resampling kernels unless the
+        // step follows a recorded ancestry without comparing
+        const int own = res;
+        const int run = a.replay_flags == nullptr || a.compare ? own : 0;
         if (a.replay_flags != nullptr)
             res = rflag != 0;
         a.hist_ess[a.t] = ess;
@@ -663,8 +668,8 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
             a.hist_mean_x[a.t] = ax1 + r[2] / S1;
             a.hist_mean_y[a.t] = ay1 + r[3] / S1;
         }
-        a.rctl->active = a.replay_flags != nullptr ? 0 : res;
-        sh_res = a.replay_flags != nullptr ? 0 : res;
+        a.rctl->active = run;
+        sh_res = run;
         sh_coeff = __ddiv_rn(1.0, S1);
     }
     __syncthreads();
@@ -721,12 +726,24 @@ k_cv_finalize(FinalizeArgs a)
 // Monitor of a step that resampled and has no following move yet:
 // (1/N) sum_i x[copy_from[i]] (set_equal_weight then ISIntegrate), plus the
 // anchor of the mixed form.
+// Both kernels return at once unless step t resampled and its gathered
+// monitor is not yet written (the decision is read on the device, so the
+// host enqueues them without a round trip).
+__device__ __forceinline__ bool monitor_pending(const FilterCtl *ctl,
+                                                long long t)
+{
+    return ctl->resampled && ctl->monitor_done != t;
+}
+
 template <typename Real>
 __global__ void __launch_bounds__(kThreads)
 k_cv_monitor_gather(const Real *x, const Real *y, const int32_t *copy_from,
-                    long long N, double *part)
+                    long long N, double *part, const FilterCtl *ctl,
+                    long long t)
 {
     __shared__ double sh[2][kThreads / 32];
+    if (!monitor_pending(ctl, t))
+        return;
     double gx = 0.0, gy = 0.0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
          i += (long long)gridDim.x * blockDim.x) {
@@ -758,7 +775,7 @@ static __global__ void k_cv_monitor_finish(const double *part, int nparts,
                                     const double *anchor_y,
                                     double *hist_mean_x, double *hist_mean_y)
 {
-    if (threadIdx.x != 0)
+    if (threadIdx.x != 0 || !monitor_pending(ctl, t))
         return;
     double tx = 0.0, ty = 0.0;
     for (int i = 0; i < nparts; ++i) {

@@ -1226,6 +1226,7 @@ int vsmc_cuda_gmm_iterate(vsmc_cuda_gmm *g, uint64_t num)
         fa.sys = is_sys(scheme);
         fa.eng = g->eng;
         fa.replay_flags = nullptr;
+        fa.compare = 0;
         const size_t fin_smem = g->ntiles <= kFinalSmemTiles
                                     ? (size_t)g->ntiles * sizeof(double)
                                     : 0;

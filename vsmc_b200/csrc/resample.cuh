@@ -1339,14 +1339,16 @@ struct ResampleWorkspace {
     int32_t *sinc;         // N (tile-local surplus counts)
 };
 
-inline int resample_ntiles(long long N)
+constexpr int resample_ntiles(long long N)
 {
     return (int)((N + kTile - 1) / kTile);
 }
 
-inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
-inline size_t resample_workspace_bytes(long long N)
+// Bytes carve_workspace lays out for N particles (constexpr so that a static
+// scratch array can be sized from it at compile time).
+constexpr size_t resample_workspace_bytes(long long N)
 {
     const size_t nt = (size_t)resample_ntiles(N) + 1;
     return align256(sizeof(ResampleCtl)) + 6 * align256(nt * 8) +

@@ -30,16 +30,17 @@ int cuda_status(cudaError_t e, const char *what);
 
 namespace {
 
-// resample_workspace_bytes(N) plus the int32 copy_from scratch used when the
-// caller passes no copy_from array.
+// The workspace carve_workspace lays out for the largest N, plus the int32
+// copy_from scratch used when the caller passes no copy_from array.  Both
+// come from the same constexpr size functions the workspace path uses, so a
+// change of the workspace layout resizes the array with it.
 constexpr long long kNoallocMaxN = VSMC_CUDA_NOALLOC_MAX_N;
-constexpr size_t kNoallocNt = (size_t)((kNoallocMaxN + kTile - 1) / kTile) + 1;
-constexpr size_t kAlign = 256;
-constexpr size_t al(size_t b) { return (b + kAlign - 1) / kAlign * kAlign; }
+constexpr size_t kNoallocCopyFromOffset = resample_workspace_bytes(kNoallocMaxN);
 constexpr size_t kNoallocBytes =
-    al(sizeof(ResampleCtl)) + 6 * al(kNoallocNt * 8) + 5 * al(kNoallocNt * 4) +
-    al(((size_t)kNoallocMaxN / 8 + 2) * 4) + al((size_t)kNoallocMaxN * 8) +
-    al((size_t)kNoallocMaxN * 4) + al((size_t)kNoallocMaxN * 4);
+    kNoallocCopyFromOffset + align256((size_t)kNoallocMaxN * 4);
+// Smaller N needs no more: the layout grows with N.
+static_assert(resample_workspace_bytes(1) <= kNoallocCopyFromOffset,
+              "workspace layout must grow with N");
 
 // In host code this name is only a stand-in for the symbol; its device
 // address comes from cudaGetSymbolAddress on each device.
@@ -48,9 +49,33 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 void *g_noalloc_ptr[kMaxDevices] = {};
+void *g_noalloc_ctx[kMaxDevices] = {}; // the context the address belongs to
+
+// cuCtxGetCurrent through the runtime's driver entry point (no link against
+// libcuda): the current context identifies the module instance the cached
+// address belongs to.  After cudaDeviceReset the device's primary context is
+// a new one, the module is loaded again and the symbol may move.
+typedef int (*CtxGetCurrentFn)(void **);
+
+void *current_context()
+{
+    static CtxGetCurrentFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault,
+                                    &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(p);
+    }();
+    void *ctx = nullptr;
+    if (fn == nullptr || fn(&ctx) != 0)
+        return nullptr;
+    return ctx;
+}
 
 // Device address of the scratch array on the current device, looked up
-// once per device (with that device current) and cached.
+// once per device and context (with that device current) and cached.
 int noalloc_scratch(void **out)
 {
     int dev = 0;
@@ -61,8 +86,13 @@ int noalloc_scratch(void **out)
         set_last_error("vsmc_cuda_resample_noalloc: device index out of range");
         return VSMC_CUDA_EINVAL;
     }
+    // (no context is current before the process's first runtime call that
+    // needs one; the lookup below creates it, and the next call then finds
+    // the context and looks the address up once more)
+    void *ctx = current_context();
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (g_noalloc_ptr[dev] == nullptr) {
+    if (g_noalloc_ptr[dev] == nullptr || ctx == nullptr ||
+        ctx != g_noalloc_ctx[dev]) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess)
@@ -70,6 +100,7 @@ int noalloc_scratch(void **out)
                                "vsmc_cuda_resample_noalloc: "
                                "cudaGetSymbolAddress");
         g_noalloc_ptr[dev] = p;
+        g_noalloc_ctx[dev] = ctx != nullptr ? ctx : current_context();
     }
     *out = g_noalloc_ptr[dev];
     return VSMC_CUDA_OK;
@@ -111,7 +142,7 @@ extern "C" int vsmc_cuda_resample_noalloc(int scheme, uint64_t N,
     int32_t *cf = copy_from;
     if (cf == nullptr)
         cf = reinterpret_cast<int32_t *>(static_cast<char *>(scratch) +
-                                         resample_workspace_bytes((long long)N));
+                                         kNoallocCopyFromOffset);
     // the control block starts from the host's values on every call
     ResampleCtl h;
     std::memset(&h, 0, sizeof(h));
