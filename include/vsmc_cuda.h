@@ -306,6 +306,100 @@ int vsmc_cuda_cv_resample_words(vsmc_cuda_cv_filter *f, uint64_t *words);
 int vsmc_cuda_cv_copy_from(vsmc_cuda_cv_filter *f, int32_t *copy_from,
                            int32_t *resampled);
 
+/* ---- the model-independent core of a device Sampler ---------------------
+ *
+ * For particle moves the caller compiles itself (nvcc, sm_100a) against
+ * include/vsmc_b200/smc_device.cuh; include/vsmc_b200/smc.cuh wraps it as
+ * vsmc::Sampler<T> with MoveCUDA / InitializeCUDA / MonitorEvalCUDA
+ * functors.  The core holds what the reference's Sampler<T> keeps apart from
+ * the value: the WeightSet (core/weight_set.hpp:96-454) as raw device
+ * log-weights, the resample engine and Particle::resample's copy_from
+ * (core/particle.hpp:230-250), and the ESS / resampled / accept histories
+ * (core/sampler.hpp:725-741).  A step is the caller's kernels followed by
+ * vsmc_cuda_smc_finish_step: normalisation, ESS, the log-evidence increment
+ * (example/include/move_smc.hpp:63-71), the decision ESS < threshold * N
+ * and the scheme's resampling, all on the device.
+ *
+ * Contract of a step's move kernel (what vsmc_cuda_smc_step describes): for
+ * every particle i, with parent p = copy_from[i] if *resampled (the previous
+ * step resampled; 0 <= p < N) else i, the move reads the parent's state,
+ * writes particle i's new state, and sets log_weight[i] to
+ *   (the previous step's log-weight, 0 after a resampling, else
+ *    log_weight[i] - *lw_max) + the step's log-weight increment,
+ * and writes one vsmc_b200::TileStats per tile of VSMC_CUDA_SMC_TILE
+ * particles (the online log-sum-exp of its new log-weights).  The first step
+ * (iter 0, Sampler::initialize) sets log_weight[i] to its increment. */
+#define VSMC_CUDA_SMC_TILE 2048     /* particles per TileStats */
+#define VSMC_CUDA_SMC_MAX_QUEUE 16  /* accept counters per step */
+
+typedef struct vsmc_cuda_smc vsmc_cuda_smc;
+
+typedef struct {
+    uint64_t N;               /* particles */
+    uint64_t ntiles;          /* tiles of VSMC_CUDA_SMC_TILE particles */
+    uint64_t iter;            /* the step the next kernels compute */
+    double *log_weight;       /* N raw log-weights (device) */
+    const double *lw_max;     /* device: maximum raw log-weight of the last
+                                 finished step (subtracted when it did not
+                                 resample: WeightSet's max-normalisation) */
+    const double *weight_s1;  /* device: sum exp(lw - lw_max) of that step */
+    const int32_t *resampled; /* device flag: the last finished step
+                                 resampled */
+    const int32_t *copy_from; /* device: N parents of that resampling */
+    void *tile_stats;         /* device: ntiles vsmc_b200::TileStats */
+    uint64_t *accept;         /* device counters, step t, queue position k:
+                                 accept[t * VSMC_CUDA_SMC_MAX_QUEUE + k]
+                                 (Sampler::accept_history) */
+    void *stream;             /* the core's cudaStream_t */
+} vsmc_cuda_smc_step;
+
+/* Sampler<T>(N, scheme, threshold)'s weight set and resampling for up to
+ * T_max steps; the resample engine is Threefry4x64(resample_seed) (the
+ * reference seeds it with the Seed::get() after the particle engines').
+ * All device memory is allocated here. */
+int vsmc_cuda_smc_create(uint64_t N, uint64_t T_max, int scheme,
+                         double threshold, uint32_t resample_seed,
+                         void *stream, vsmc_cuda_smc **out);
+int vsmc_cuda_smc_destroy(vsmc_cuda_smc *s);
+
+/* Sampler::initialize's reset (core/sampler.hpp:764-776): step 0, equal
+ * weights, histories and accept counters cleared, running log-evidence 0;
+ * the resample engine keeps its position.  Asynchronous. */
+int vsmc_cuda_smc_reset(vsmc_cuda_smc *s);
+
+/* The device pointers and step number a move kernel of the next step uses. */
+int vsmc_cuda_smc_step_args(vsmc_cuda_smc *s, vsmc_cuda_smc_step *out);
+
+/* Ends the step the kernels computed: Sampler::do_resample
+ * (core/sampler.hpp:816-822) on the device.  Asynchronous. */
+int vsmc_cuda_smc_finish_step(vsmc_cuda_smc *s);
+
+/* Waits for the core's stream; reports sticky device errors. */
+int vsmc_cuda_smc_synchronize(vsmc_cuda_smc *s);
+
+int vsmc_cuda_smc_iter_size(vsmc_cuda_smc *s, uint64_t *iter_size);
+
+/* Histories of the finished steps (host arrays of iter_size entries; accept
+ * has iter_size x VSMC_CUDA_SMC_MAX_QUEUE; each may be NULL): ESS,
+ * resampled flags, log-evidence increments, accept counts.  Synchronises. */
+int vsmc_cuda_smc_history(vsmc_cuda_smc *s, double *ess, int32_t *resampled,
+                          double *logz_inc, uint64_t *accept);
+
+/* Running log-evidence sum.  Synchronises. */
+int vsmc_cuda_smc_log_evidence(vsmc_cuda_smc *s, double *logz);
+
+/* WeightSet::read_weight / read_log_weight after the last step (equal
+ * weights when it resampled); host arrays of N, each may be NULL.
+ * Synchronises. */
+int vsmc_cuda_smc_read_weights(vsmc_cuda_smc *s, double *weight,
+                               double *log_weight);
+
+/* Words drawn so far by the resample engine. */
+int vsmc_cuda_smc_resample_words(vsmc_cuda_smc *s, uint64_t *words);
+
+/* Kernel launches the core has issued. */
+int vsmc_cuda_smc_launches(vsmc_cuda_smc *s, uint64_t *launches);
+
 /* ---- many filters on one device (batched runs and serving) -------------
  *
  * No counterpart in the reference, which runs one Sampler per filter

@@ -403,6 +403,41 @@ def ref_cv_summary(N, T, scheme, obs_x, obs_y, seed=101, stream=0, threshold=0.5
     return buf.value.decode()
 
 
+PAPER_REF_SO = os.path.join(HERE, "_ref", "libvsmc_paper_ref.so")
+
+
+def paper_ref_available() -> bool:
+    return os.path.exists(PAPER_REF_SO)
+
+
+def ref_paper_pf_summary(N, T, obs_x, obs_y, seed=101) -> str:
+    """`os << sampler` of the reference's example/paper particle filter
+    (paper_pf.cpp's own cv, cv_init, cv_move and monitor, Stratified at
+    ESS < N/2, through vSMC's Sampler) on the given observations, which are
+    written to the 100-row data file the example reads."""
+    import tempfile
+
+    L = C.CDLL(PAPER_REF_SO)
+    L.ref_paper_pf_summary.restype = C.c_uint64
+    L.ref_paper_pf_summary.argtypes = [C.c_uint64, C.c_uint64, C.c_uint, C.c_char_p,
+                                       C.c_char_p, C.c_uint64]
+    ox = np.zeros(100)
+    oy = np.zeros(100)
+    ox[:len(obs_x)] = obs_x
+    oy[:len(obs_y)] = obs_y
+    fd, path = tempfile.mkstemp(suffix=".data")
+    try:
+        with os.fdopen(fd, "w") as f:
+            for a, b in zip(ox, oy):
+                f.write(f"{float(a)!r} {float(b)!r}\n")
+        n = L.ref_paper_pf_summary(N, T, seed, path.encode(), None, 0)
+        buf = C.create_string_buffer(int(n) + 1)
+        L.ref_paper_pf_summary(N, T, seed, path.encode(), buf, int(n) + 1)
+    finally:
+        os.unlink(path)
+    return buf.value.decode()
+
+
 def ref_max_threads() -> int:
     return ref().ref_max_threads()
 

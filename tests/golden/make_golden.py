@@ -6,7 +6,9 @@ Run from the repository root where the vSMC include tree is available:
 
 (`python tests/golden/make_golden.py summaries` rewrites only the summary
 tables cv_summary_s*.tsv; `... gmm` only gmm.npz and gmm_summary.tsv, the
-tempered SMC sampler of oracle/ref_gmm.cpp.)
+tempered SMC sampler of oracle/ref_gmm.cpp; `... paper` only
+paper_pf_obs.npz and paper_pf_summary.tsv, the reference's example/paper
+particle filter of oracle/ref_paper_pf.cpp.)
 
 Every array in golden.npz is produced by oracle/_ref/libvsmc_ref.so
 (oracle/ref_harness.cpp over vSMC's own Sampler, WeightSet, Resample<...>,
@@ -165,11 +167,32 @@ def write_gmm():
         f.write(text)
 
 
+PAPER_RUN = dict(N=1000, T=100, seed=101, obs_seed=11)
+
+
+def write_paper():
+    """paper_pf_summary.tsv: `os << sampler` of the reference's
+    example/paper/src/paper_pf.cpp model (its own classes, Stratified at
+    ESS < N/2, Threefry4x64 engine per particle slot) on the workload's
+    simulated series (obs seed 11), saved in paper_pf_obs.npz."""
+    here = os.path.dirname(os.path.abspath(__file__))
+    ox, oy = O.cv_simulate(PAPER_RUN["T"], obs_seed=PAPER_RUN["obs_seed"])
+    text = O.ref_paper_pf_summary(PAPER_RUN["N"], PAPER_RUN["T"], ox, oy,
+                                  seed=PAPER_RUN["seed"])
+    np.savez_compressed(os.path.join(here, "paper_pf_obs.npz"), obs_x=ox, obs_y=oy,
+                        **{k: np.array(v) for k, v in PAPER_RUN.items()})
+    with open(os.path.join(here, "paper_pf_summary.tsv"), "w") as f:
+        f.write(text)
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["gmm"]:
         write_gmm()
+    elif sys.argv[1:] == ["paper"]:
+        write_paper()
     else:
         if sys.argv[1:] != ["summaries"]:
             main()
             write_gmm()
+            write_paper()
         write_summaries()

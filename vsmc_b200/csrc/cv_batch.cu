@@ -118,15 +118,16 @@ __global__ void __launch_bounds__(kMoveThreads, MinBlocks * 256 / kMoveThreads)
 kb_move(const BatchSlot *slots, const TileRef *map, CVParam p)
 {
     __shared__ double sh_w[7 * kMoveWarps];
+    extern __shared__ double2 pts[]; // kPolarSmemBytes
     const TileRef r = map[blockIdx.x];
     const BatchSlot &b = slots[r.slot];
     const MoveArgs<Real> a = batch_move_args<Real>(b, p);
     if (a.iter == 0) {
         const MoveStep<Real> ms = move_step<Real, true>(a);
-        cv_move_tile<Real, true>(a, ms, r.tile, sh_w);
+        cv_move_tile<Real, true>(a, ms, r.tile, sh_w, pts);
     } else {
         const MoveStep<Real> ms = move_step<Real, false>(a);
-        cv_move_tile<Real, false>(a, ms, r.tile, sh_w);
+        cv_move_tile<Real, false>(a, ms, r.tile, sh_w, pts);
     }
 }
 
@@ -628,13 +629,16 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
     const int32_t *work = b->d_work;
     switch (b->tune_move) {
     case 2:
-        kb_move<Real, 2><<<nt, kMoveThreads, 0, s>>>(sl, map, b->bc.p);
+        kb_move<Real, 2><<<nt, kMoveThreads, kPolarSmemBytes, s>>>(
+            sl, map, b->bc.p);
         break;
     case 4:
-        kb_move<Real, 4><<<nt, kMoveThreads, 0, s>>>(sl, map, b->bc.p);
+        kb_move<Real, 4><<<nt, kMoveThreads, kPolarSmemBytes, s>>>(
+            sl, map, b->bc.p);
         break;
     default:
-        kb_move<Real, 3><<<nt, kMoveThreads, 0, s>>>(sl, map, b->bc.p);
+        kb_move<Real, 3><<<nt, kMoveThreads, kPolarSmemBytes, s>>>(
+            sl, map, b->bc.p);
         break;
     }
     // a finalize CTA narrower than 1024 threads gives the same sums only
@@ -775,6 +779,21 @@ int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
     if (b == nullptr)
         return VSMC_CUDA_ENOMEM;
     b->model = *model;
+    {
+        const int sm = (int)kPolarSmemBytes;
+        cudaFuncSetAttribute(kb_move<double, 2>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(kb_move<double, 3>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(kb_move<double, 4>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(kb_move<float, 2>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(kb_move<float, 3>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(kb_move<float, 4>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    }
     b->bc.p = cv_param(*model);
     b->bc.threshold = model->threshold;
     b->bc.residual = is_residual(model->scheme);

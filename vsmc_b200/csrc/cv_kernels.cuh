@@ -28,13 +28,6 @@ struct FilterCtl {
     long long monitor_done; // step whose gathered monitor is already written
 };
 
-// Per-tile statistics of the new log-weights: online log-sum-exp (m, s1, s2),
-// the weighted position sums (sx, sy) and the sums of the gathered previous
-// positions (gx, gy) for the monitor of a resampled step.
-struct TileStats {
-    double m, s1, s2, sx, sy, gx, gy, pad;
-};
-
 struct CVParam {
     double dt, sd_pos, sd_vel, sd_pos0, sd_vel0, scale, nu;
     double inv_nu; // 1 / nu
@@ -88,19 +81,31 @@ __device__ __forceinline__ PhiloxStream particle_stream(uint32_t iter,
     return s;
 }
 
+// The two accepted polar points of one particle's step (libstdc++'s two
+// calls of the polar loop), drawn by polar_points_tile.  r2 = x^2 + y^2 is
+// recomputed with the same two products and sum, so it is the value the
+// acceptance test saw.
+struct PolarPair {
+    double x1, y1, x2, y2;
+};
+
+__device__ __forceinline__ double polar_r2(double x, double y)
+{
+    return __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+}
+
 // FP64 form: cv_move::move_state / cv_init::initialize_state
-// (pf_smp.hpp:150-173, 207-238).  The two polar points are drawn first and
-// their transforms evaluated together (independent chains for the FP64
-// pipe); the state update keeps the reference's evaluation order.
+// (pf_smp.hpp:150-173, 207-238).  The two polar transforms are evaluated
+// together (independent chains for the FP64 pipe); the state update keeps
+// the reference's evaluation order.
 template <bool Init>
-__device__ __forceinline__ void cv_particle(const CVParam &p, uint32_t iter,
-                                            uint32_t id, uint32_t stream,
-                                            uint32_t k0, uint32_t k1,
-                                            double &x, double &y, double &vx,
+__device__ __forceinline__ void cv_particle(const CVParam &p,
+                                            const PolarPair &pp, double &x,
+                                            double &y, double &vx,
                                             double &vy, double, double)
 {
-    double x1, y1, q1, x2, y2, q2;
-    polar_two(iter, id, stream, k0, k1, x1, y1, q1, x2, y2, q2);
+    const double x1 = pp.x1, y1 = pp.y1, x2 = pp.x2, y2 = pp.y2;
+    const double q1 = polar_r2(x1, y1), q2 = polar_r2(x2, y2);
     const double m1 = polar_mult_f64(q1);
     const double m2 = polar_mult_f64(q2);
     const double a = __dmul_rn(y1, m1), b = __dmul_rn(x1, m1);
@@ -139,14 +144,13 @@ __device__ __forceinline__ double cv_loglik(const CVParam &p, double x,
 // residual); (shx, shy) = previous observation minus this one, in double
 // rounded once, re-anchors the loaded offsets.
 template <bool Init>
-__device__ __forceinline__ void cv_particle(const CVParam &p, uint32_t iter,
-                                            uint32_t id, uint32_t stream,
-                                            uint32_t k0, uint32_t k1, float &x,
+__device__ __forceinline__ void cv_particle(const CVParam &p,
+                                            const PolarPair &pp, float &x,
                                             float &y, float &vx, float &vy,
                                             double shx, double shy)
 {
-    double x1, y1, q1, x2, y2, q2;
-    polar_two(iter, id, stream, k0, k1, x1, y1, q1, x2, y2, q2);
+    const double x1 = pp.x1, y1 = pp.y1, x2 = pp.x2, y2 = pp.y2;
+    const double q1 = polar_r2(x1, y1), q2 = polar_r2(x2, y2);
     if (Init) {
         // once per run: the prior in double, then stored as float offsets
         const double m1 = polar_mult_f64(q1), m2 = polar_mult_f64(q2);
@@ -172,97 +176,6 @@ __device__ __forceinline__ float cv_loglik(const CVParam &p, float x, float y,
     const float lx = s * x, ly = s * y;
     const float a = lx * lx * inv, b = ly * ly * inv;
     return (float)p.coef * log1pf(a + b + a * b);
-}
-
-__device__ __forceinline__ double lse_exp(double v) { return exp(v); }
-__device__ __forceinline__ double lse_exp(float v) { return (double)expf(v); }
-
-// Per-thread weight statistics against a lazy reference: the first finite
-// log-weight becomes the reference and later values are accumulated as
-// exp(lw - ref) even above it (double has the range), so the exponential is
-// evaluated once per particle; the reference moves only when a value
-// exceeds it by more than kLazy (then exp^2 could overflow).  mx tracks the
-// true maximum.
-struct LseRef {
-    double ref, mx, s1, s2, sx, sy;
-
-    __device__ __forceinline__ void init()
-    {
-        ref = -INFINITY;
-        mx = -INFINITY;
-        s1 = s2 = sx = sy = 0.0;
-    }
-};
-
-template <typename Real>
-struct LazyBound;
-template <>
-struct LazyBound<double> {
-    static constexpr double v = 300.0;
-};
-template <>
-struct LazyBound<float> {
-    static constexpr double v = 40.0;
-};
-
-template <typename Real>
-__device__ __forceinline__ void lse_add(LseRef &a, Real lw, Real x, Real y)
-{
-    const double l = (double)lw;
-    if (l != l) {
-        a.s1 = l; // NaN propagates to the degenerate check
-        return;
-    }
-    if (l == -INFINITY)
-        return;
-    a.mx = fmax(a.mx, l);
-    if (a.ref == -INFINITY) {
-        a.ref = l;
-    } else if (l - a.ref > LazyBound<Real>::v) {
-        const double f = exp(a.ref - l);
-        a.s1 *= f;
-        a.s2 *= f * f;
-        a.sx *= f;
-        a.sy *= f;
-        a.ref = l;
-    }
-    const double e = lse_exp((Real)(lw - (Real)a.ref));
-    a.s1 += e;
-    a.s2 += e * e;
-    a.sx += e * (double)x;
-    a.sy += e * (double)y;
-}
-
-// Rescale a thread's sums to the common maximum M: exp(ref - M) <= 1.
-__device__ __forceinline__ void lse_rescale(LseRef &a, double M)
-{
-    const double f = a.ref == -INFINITY ? 0.0 : exp(a.ref - M);
-    a.s1 *= f;
-    a.s2 *= f * f;
-    a.sx *= f;
-    a.sy *= f;
-    a.ref = M;
-}
-
-__device__ __forceinline__ double warp_max_nan(double v, unsigned width)
-{
-    for (unsigned o = width / 2; o > 0; o >>= 1)
-        v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
-// Sum of the rescaled statistics over `width` lanes.
-__device__ __forceinline__ void warp_sum_stats(LseRef &a, double &gx,
-                                               double &gy, unsigned width)
-{
-    for (unsigned o = width / 2; o > 0; o >>= 1) {
-        a.s1 += __shfl_xor_sync(0xffffffffu, a.s1, o);
-        a.s2 += __shfl_xor_sync(0xffffffffu, a.s2, o);
-        a.sx += __shfl_xor_sync(0xffffffffu, a.sx, o);
-        a.sy += __shfl_xor_sync(0xffffffffu, a.sy, o);
-        gx += __shfl_xor_sync(0xffffffffu, gx, o);
-        gy += __shfl_xor_sync(0xffffffffu, gy, o);
-    }
 }
 
 #ifndef VSMC_MOVE_MIN_BLOCKS
@@ -303,26 +216,91 @@ constexpr int kMoveThreads = 256;                 // threads of a move CTA
 constexpr int kMoveItems = kTile / kMoveThreads; // particles per thread
 constexpr int kMoveWarps = kMoveThreads / 32;
 
+// Shared memory a move CTA needs for its polar points: two (x, y) pairs
+// for each of its kTile particles (64 KiB).
+constexpr size_t kPolarSmemBytes = (size_t)kTile * 2 * sizeof(double2);
+
+// Phase 1 of a move tile: the polar points of the thread's kMoveItems
+// particles.  A particle's points come from its own Philox4x32-10 stream
+// (counter {block, step, id, stream}, block = 1, 2, ...), one block per
+// polar attempt, and the polar method (libstdc++ normal_distribution)
+// keeps the first two attempts with 0 < x^2 + y^2 <= 1.  The thread walks
+// its particles one after another through a single loop of one block per
+// iteration, so a warp runs for the largest total number of attempts of a
+// lane (about 25 for 8 particles, 2.55 expected per particle) instead of
+// paying the slowest lane's rejection tail once per particle (about 4.8
+// blocks per particle).  Each particle's points are the same as the
+// sequential loop's, in stream order.  `pts` is the thread's slice:
+// slot (2 j + k) * kMoveThreads + threadIdx.x holds point k of the thread's
+// j-th particle; only this thread reads it back, so no barrier is needed.
+template <int V>
+__device__ __forceinline__ void polar_points_tile(uint32_t iter,
+                                                  uint32_t stream,
+                                                  uint32_t k0, uint32_t k1,
+                                                  long long base, long long N,
+                                                  double2 *pts)
+{
+    // the thread's j-th particle: pass v = j / V, element e = j % V
+    auto pid = [&](int j) {
+        return base + ((long long)(j / V) * kMoveThreads + threadIdx.x) * V +
+               (j % V);
+    };
+    long long id = pid(0);
+    if (id >= N)
+        return;
+    PhiloxStream s;
+    s.ctr = make_uint4(0u, iter, (uint32_t)id, stream);
+    s.k0 = k0;
+    s.k1 = k1;
+    int j = 0, k = 0;
+#pragma unroll 1
+    while (true) {
+        double x, y, r2;
+        polar_point(s.next_block(), x, y, r2);
+        if (polar_ok(r2)) {
+            pts[(2 * j + k) * kMoveThreads + threadIdx.x] = make_double2(x, y);
+            if (++k == 2) {
+                k = 0;
+                if (++j == kMoveItems)
+                    break;
+                id = pid(j);
+                if (id >= N)
+                    break;
+                s.ctr = make_uint4(0u, iter, (uint32_t)id, stream);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ PolarPair polar_pair(const double2 *pts, int j)
+{
+    const double2 a = pts[(2 * j) * kMoveThreads + threadIdx.x];
+    const double2 b = pts[(2 * j + 1) * kMoveThreads + threadIdx.x];
+    return PolarPair{a.x, a.y, b.x, b.y};
+}
+
 // One tile of kTile particles: load (gather), move, likelihood, log-weight
 // update and the tile's online log-sum-exp statistics.  `sh_w` holds
 // 7 x kMoveWarps warp partials; a CTA alternates two such buffers so that
-// one barrier per tile suffices.
+// one barrier per tile suffices.  `pts` is kPolarSmemBytes of shared memory
+// for the polar points (phase 1), which the move (phase 2) consumes.
 template <typename Real, bool Init>
 __device__ __forceinline__ void cv_move_tile(const MoveArgs<Real> &a,
                                              const MoveStep<Real> &ms,
-                                             int tile, double *sh_w)
+                                             int tile, double *sh_w,
+                                             double2 *pts)
 {
     constexpr int V = Vec<Real>::n;
     constexpr int NV = kMoveItems / V;
     typedef typename Vec<Real>::type VT;
     constexpr int NW = kMoveWarps;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int gather = ms.gather;
     const Real mprev = ms.mprev;
     const double ox = ms.ox, oy = ms.oy, shx = ms.shx, shy = ms.shy;
     const long long N = a.N;
     {
         const long long base = (long long)tile * kTile;
+        polar_points_tile<V>(a.iter, a.stream, a.k0, a.k1, base, N, pts);
         LseRef acc;
         acc.init();
         double gx = 0.0, gy = 0.0;
@@ -375,9 +353,8 @@ __device__ __forceinline__ void cv_move_tile(const MoveArgs<Real> &a,
             for (int e = 0; e < V; ++e) {
                 const long long i = p0 + e;
                 if (i < N) {
-                    cv_particle<Init>(a.p, a.iter, (uint32_t)i, a.stream, a.k0,
-                                      a.k1, s[0][e], s[1][e], s[2][e],
-                                      s[3][e], shx, shy);
+                    cv_particle<Init>(a.p, polar_pair(pts, v * V + e), s[0][e],
+                                      s[1][e], s[2][e], s[3][e], shx, shy);
                     const Real inc = cv_loglik(a.p, s[0][e], s[1][e], ox, oy);
                     // lw += -max (normalize_log_weight), then += inc
                     lwn[e] = Init ? inc : (lwv[e] - mprev) + inc;
@@ -413,52 +390,7 @@ __device__ __forceinline__ void cv_move_tile(const MoveArgs<Real> &a,
                 }
             }
         }
-        // warp: common maximum, one rescale per lane, plain sums
-        const double wm = warp_max_nan(acc.mx, 32);
-        lse_rescale(acc, wm);
-        warp_sum_stats(acc, gx, gy, 32);
-        if (lane == 0) {
-            double *w = sh_w;
-            w[0 * NW + wid] = wm;
-            w[1 * NW + wid] = acc.s1;
-            w[2 * NW + wid] = acc.s2;
-            w[3 * NW + wid] = acc.sx;
-            w[4 * NW + wid] = acc.sy;
-            w[5 * NW + wid] = gx;
-            w[6 * NW + wid] = gy;
-        }
-        __syncthreads();
-        if (wid == 0) {
-            const double *w = sh_w;
-            LseRef r;
-            double tx = 0.0, ty = 0.0;
-            r.init();
-            if (lane < NW) {
-                r.ref = w[0 * NW + lane];
-                r.mx = r.ref;
-                r.s1 = w[1 * NW + lane];
-                r.s2 = w[2 * NW + lane];
-                r.sx = w[3 * NW + lane];
-                r.sy = w[4 * NW + lane];
-                tx = w[5 * NW + lane];
-                ty = w[6 * NW + lane];
-            }
-            const double tm = warp_max_nan(r.mx, NW);
-            lse_rescale(r, tm);
-            warp_sum_stats(r, tx, ty, NW);
-            if (lane == 0) {
-                TileStats ts;
-                ts.m = tm;
-                ts.s1 = r.s1;
-                ts.s2 = r.s2;
-                ts.sx = r.sx;
-                ts.sy = r.sy;
-                ts.gx = tx;
-                ts.gy = ty;
-                ts.pad = 0.0;
-                a.tile_stats[tile] = ts;
-            }
-        }
+        tile_stats_reduce<NW>(acc, gx, gy, sh_w, a.tile_stats + tile);
     }
 }
 
@@ -469,12 +401,32 @@ k_cv_move(MoveArgs<Real> a)
 {
     // double-buffered warp partials: one barrier per tile
     __shared__ double sh_w[2][7 * kMoveWarps];
+    extern __shared__ double2 pts[]; // kPolarSmemBytes
     const MoveStep<Real> ms = move_step<Real, Init>(a);
     int buf = 0;
     for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        cv_move_tile<Real, Init>(a, ms, tile, sh_w[buf]);
+        cv_move_tile<Real, Init>(a, ms, tile, sh_w[buf], pts);
         buf ^= 1;
     }
+}
+
+// The move kernels take kPolarSmemBytes of dynamic shared memory (above
+// the 48 KiB default); set once per device before their first launch.
+inline cudaError_t set_move_smem_attributes()
+{
+    const int b = (int)kPolarSmemBytes;
+    cudaError_t e = cudaFuncSetAttribute(
+        k_cv_move<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_cv_move<double, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_cv_move<float, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_cv_move<float, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    return e;
 }
 
 struct FinalizeArgs {
