@@ -107,6 +107,22 @@ typedef struct {
 int vsmc_cuda_weight_add_log(uint64_t N, double *log_weight, double *weight,
                              const double *inc, double *ess, void *stream);
 
+/* WeightSet::ess(first, use_log) (core/weight_set.hpp:132-146 and
+ * compute_ess :385-409): the ESS the weights would have after an update by
+ * the N incremental weights `inc` (device), without changing them.  With
+ * use_log, inc are log increments added to the max-normalised log_weight;
+ * otherwise inc multiply the normalised `weight`.  Blocks. */
+int vsmc_cuda_weight_ess(uint64_t N, const double *log_weight,
+                         const double *weight, const double *inc, int use_log,
+                         double *ess, void *stream);
+
+/* WeightSet::cess(first, use_log) (core/weight_set.hpp:160-174 and
+ * compute_cess :411-431): the conditional ESS (sum W b)^2 / sum W b^2 of the
+ * normalised `weight` and the incremental weights b = inc (or exp(inc) with
+ * use_log), device arrays of N.  Blocks. */
+int vsmc_cuda_weight_cess(uint64_t N, const double *weight, const double *inc,
+                          int use_log, double *cess, void *stream);
+
 /* ----------------------------------------------------------- resample --- */
 
 /* Bytes of device workspace vsmc_cuda_resample needs for N particles. */
@@ -130,6 +146,25 @@ int vsmc_cuda_resample(int scheme, uint64_t N, const double *weight,
                        vsmc_cuda_threefry_state *rng, int32_t *replication,
                        int32_t *copy_from, void *workspace,
                        size_t workspace_bytes, void *stream);
+
+/* Bytes of device workspace vsmc_cuda_resample_mn needs. */
+size_t vsmc_cuda_resample_mn_workspace_size(uint64_t M, uint64_t N);
+
+/* Resample<Scheme>::operator()(M, N, rng, weight, replication) followed by
+ * internal::cfrp_trans(M, N, replication, copy_from) for M weights and N
+ * children (resample/*.hpp; common.hpp:57-118): replication has M entries
+ * summing to N; copy_from (N entries, may be NULL) is, for M != N, the
+ * cfrp_trans expansion (parent i repeated replication[i] times, in order)
+ * and for M == N the same as vsmc_cuda_resample.  M >= 1; N = 0 leaves every
+ * count at zero (a Systematic engine still draws its one word).  uniforms /
+ * n_uniforms as vsmc_cuda_resample, with up to N values.  The engine
+ * advances by exactly the words the reference draws.  Blocks until done. */
+int vsmc_cuda_resample_mn(int scheme, uint64_t M, uint64_t N,
+                          const double *weight, const double *uniforms,
+                          uint64_t n_uniforms, vsmc_cuda_threefry_state *rng,
+                          int32_t *replication, int32_t *copy_from,
+                          void *workspace, size_t workspace_bytes,
+                          void *stream);
 
 /* Largest N accepted by vsmc_cuda_resample_noalloc. */
 #define VSMC_CUDA_NOALLOC_MAX_N 262144

@@ -200,6 +200,18 @@ def ref_weight_set(lw, inc=None):
     return ess, w, lwo
 
 
+def ref_weight_prospective(lw, inc, use_log, cess):
+    """WeightSet::set_log_weight(lw) then ess(inc, use_log) or cess(inc,
+    use_log), through vSMC."""
+    L = ref()
+    L.ref_weight_prospective.restype = C.c_double
+    L.ref_weight_prospective.argtypes = [C.c_uint64, _f64p, _f64p, C.c_int, C.c_int]
+    lw = np.ascontiguousarray(lw, np.float64)
+    inc = np.ascontiguousarray(inc, np.float64)
+    return L.ref_weight_prospective(lw.size, lw, inc, 1 if use_log else 0,
+                                    1 if cess else 0)
+
+
 # -------------------------------------------------------------- resample --
 
 def resample(scheme, weights, seed, skip=0, M=None, N=None, want_uniforms=False):

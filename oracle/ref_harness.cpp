@@ -431,6 +431,16 @@ double ref_weight_set (uint64_t N, const double *lw, const double *inc,
     return ws.ess();
 }
 
+// WeightSet::set_log_weight(lw) then ess(inc, use_log) or cess(inc,
+// use_log) (weight_set.hpp:132-186, 385-431): the prospective ESS / CESS.
+double ref_weight_prospective (uint64_t N, const double *lw, const double *inc,
+        int use_log, int cess)
+{
+    vsmc::WeightSet ws(N);
+    ws.set_log_weight(lw);
+    return cess ? ws.cess(inc, use_log != 0) : ws.ess(inc, use_log != 0);
+}
+
 // The CV Student-t bootstrap filter through Sampler<T>; backend 0 = OMP
 // (StateOMP/InitializeOMP/MoveOMP/MonitorEvalOMP), 1 = STD (std::thread),
 // 2 = SEQ.  nthreads > 0 sets the OpenMP thread count (OMP backend).

@@ -8,7 +8,9 @@ Run from the repository root where the vSMC include tree is available:
 tables cv_summary_s*.tsv; `... gmm` only gmm.npz and gmm_summary.tsv, the
 tempered SMC sampler of oracle/ref_gmm.cpp; `... paper` only
 paper_pf_obs.npz and paper_pf_summary.tsv, the reference's example/paper
-particle filter of oracle/ref_paper_pf.cpp.)
+particle filter of oracle/ref_paper_pf.cpp; `... prospective` only
+prospective.npz, WeightSet::ess / cess of incremental weights; `... mn`
+only resample_mn.npz, resampling M weights into N != M children.)
 
 Every array in golden.npz is produced by oracle/_ref/libvsmc_ref.so
 (oracle/ref_harness.cpp over vSMC's own Sampler, WeightSet, Resample<...>,
@@ -167,6 +169,52 @@ def write_gmm():
         f.write(text)
 
 
+def write_prospective():
+    """prospective.npz: WeightSet::ess(inc, use_log) and cess(inc, use_log)
+    through vSMC for log-weights and increments of several shapes, with the
+    normalised weights and log-weights WeightSet holds before the call."""
+    rng = np.random.default_rng(77)
+    g = {}
+    cases = [("small", rng.normal(size=7) * 2, rng.normal(size=7)),
+             ("wide", rng.normal(size=5000) * 5, rng.normal(size=5000) * 3),
+             ("positive", rng.normal(size=4096), rng.uniform(0.1, 2.0, size=4096)),
+             ("big", rng.normal(size=70001), rng.normal(size=70001) * 0.5)]
+    for name, lw, inc in cases:
+        _, w, lwn = O.ref_weight_set(lw)
+        g[f"{name}_lw"] = lwn
+        g[f"{name}_w"] = w
+        g[f"{name}_inc"] = inc
+        for use_log in (0, 1):
+            for cess in (0, 1):
+                g[f"{name}_{'cess' if cess else 'ess'}_{use_log}"] = np.array(
+                    O.ref_weight_prospective(lw, inc, use_log, cess))
+    np.savez_compressed(os.path.join(os.path.dirname(OUT), "prospective.npz"), **g)
+
+
+MN_CASES = ((7, 12), (1000, 1731), (4096, 100), (3000, 3), (2, 9000))
+
+
+def write_mn():
+    """resample_mn.npz: Resample<Scheme>(M, N) and cfrp_trans(M, N) with
+    M != N through vSMC (replication, copy_from, engine words) for random
+    weights, every scheme and two engine positions."""
+    rng = np.random.default_rng(5151)
+    g = {}
+    for M, N in MN_CASES:
+        lw = rng.normal(size=M) * 2.0
+        w = np.exp(lw - lw.max())
+        w /= w.sum()
+        g[f"M{M}_N{N}_w"] = w
+        for sch in range(6):
+            for seed, skip in ((103, 0), (7, 5)):
+                rep, cf, words = O.ref_resample(sch, w, seed, skip, M=M, N=N)
+                tag = f"M{M}_N{N}_s{sch}_{seed}_{skip}"
+                g[tag + "_rep"] = rep
+                g[tag + "_cf"] = cf
+                g[tag + "_words"] = np.array(words)
+    np.savez_compressed(os.path.join(os.path.dirname(OUT), "resample_mn.npz"), **g)
+
+
 PAPER_RUN = dict(N=1000, T=100, seed=101, obs_seed=11)
 
 
@@ -190,9 +238,15 @@ if __name__ == "__main__":
         write_gmm()
     elif sys.argv[1:] == ["paper"]:
         write_paper()
+    elif sys.argv[1:] == ["prospective"]:
+        write_prospective()
+    elif sys.argv[1:] == ["mn"]:
+        write_mn()
     else:
         if sys.argv[1:] != ["summaries"]:
             main()
             write_gmm()
             write_paper()
+            write_prospective()
+            write_mn()
         write_summaries()

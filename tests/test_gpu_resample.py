@@ -209,3 +209,115 @@ def test_bad_arguments(capi):
     with pytest.raises(capi.VsmcCudaError) as e:
         capi.resample(7, 10, 0, capi.threefry_state(1), None, None, None, 0)
     assert e.value.status == capi.EINVAL
+
+
+def gpu_resample_mn(capi, scheme, w, N, seed, skip, uniforms=None):
+    M = w.size
+    wd = dev(w)
+    rep = empty(M, torch.int32)
+    cf = empty(max(N, 1), torch.int32)
+    nb = capi.resample_mn_workspace_size(M, N)
+    ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    rng = capi.threefry_state(seed, offset=skip)
+    up, nu = None, 0
+    if uniforms is not None and uniforms.size > 0:
+        ud = dev(uniforms)
+        up, nu = ud.data_ptr(), uniforms.size
+    words = capi.resample_mn(scheme, M, N, wd.data_ptr(), rng, rep.data_ptr(),
+                             cf.data_ptr(), ws.data_ptr(), nb, uniforms_ptr=up, n_uniforms=nu)
+    return rep.cpu().numpy()[:M], cf.cpu().numpy()[:N], words
+
+
+def test_golden_m_ne_n_bit_exact(golden, capi):
+    """Resample(M, N) with M != N and cfrp_trans's expansion branch
+    (resample/common.hpp:110-117) on the golden cases whose N differs from
+    the number of weights."""
+    n = 0
+    for name in golden["res_names"]:
+        name = str(name)
+        w = golden[f"res_{name}_w"]
+        N = int(golden[f"res_{name}_N"])
+        if N == w.size or w.size == 0:
+            continue
+        for sch in range(6):
+            for seed, skip in ((103, 0), (7, 5)):
+                tag = f"res_{name}_s{sch}_{seed}_{skip}"
+                uni = None
+                if sch in LOG_EXP_SCHEMES:
+                    _, _, _, uni = O.resample(sch, w, seed, skip, M=w.size, N=N,
+                                              want_uniforms=True)
+                rep, cf, words = gpu_resample_mn(capi, sch, w, N, seed, skip, uni)
+                assert np.array_equal(rep, golden[tag + "_rep"]), tag
+                assert np.array_equal(cf, golden[tag + "_cf"][:N]), tag
+                assert words == int(golden[tag + "_words"]), tag
+                n += 1
+    assert n >= 12
+
+
+def test_m_ne_n_golden_bit_exact(capi):
+    """Resample(M, N) + cfrp_trans expansion against vSMC's own results
+    (tests/golden/resample_mn.npz)."""
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_golden import MN_CASES
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "resample_mn.npz"))
+    for M, N in MN_CASES:
+        w = g[f"M{M}_N{N}_w"]
+        for sch in range(6):
+            for seed, skip in ((103, 0), (7, 5)):
+                tag = f"M{M}_N{N}_s{sch}_{seed}_{skip}"
+                uni = None
+                if sch in LOG_EXP_SCHEMES:
+                    _, _, _, uni = O.resample(sch, w, seed, skip, M=M, N=N,
+                                              want_uniforms=True)
+                rep, cf, words = gpu_resample_mn(capi, sch, w, N, seed, skip, uni)
+                assert np.array_equal(rep, g[tag + "_rep"]), tag
+                assert np.array_equal(cf, g[tag + "_cf"]), tag
+                assert words == int(g[tag + "_words"]), tag
+
+
+@pytest.mark.parametrize("M,N", [(3000, (1 << 17) + 11), ((1 << 16) + 3, 5000),
+                                 (1, 777), (4097, 2)])
+@pytest.mark.parametrize("sch", range(6))
+def test_m_ne_n_against_oracle(capi, M, N, sch):
+    rng = np.random.default_rng(M + 13 * sch)
+    lw = rng.normal(size=M) * 2.0
+    w = np.exp(lw - lw.max())
+    w /= w.sum()
+    ref_rep, ref_cf, ref_words, uni = O.resample(sch, w, 19, 2, M=M, N=N,
+                                                 want_uniforms=True)
+    rep, cf, words = gpu_resample_mn(capi, sch, w, N, 19, 2,
+                                     uni if sch in LOG_EXP_SCHEMES else None)
+    assert words == ref_words
+    assert rep.sum() == N
+    assert np.array_equal(rep, ref_rep)
+    assert np.array_equal(cf, ref_cf)
+
+
+def test_m_ne_n_zero_children(capi):
+    w = np.full(10, 0.1)
+    for sch in range(6):
+        rep, cf, words = gpu_resample_mn(capi, sch, w, 0, 5, 0)
+        assert np.all(rep == 0)
+        assert words == (1 if sch in (3, 5) else 0)
+
+
+def test_prospective_ess_cess(capi):
+    """WeightSet::ess(inc, use_log) and cess(inc, use_log) against vSMC's
+    values (tests/golden/prospective.npz), relative 1e-10."""
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "prospective.npz"))
+    for name in ("small", "wide", "positive", "big"):
+        lw, w, inc = dev(g[f"{name}_lw"]), dev(g[f"{name}_w"]), dev(g[f"{name}_inc"])
+        N = g[f"{name}_lw"].size
+        for use_log in (0, 1):
+            ess = capi.weight_ess(N, lw.data_ptr(), w.data_ptr(), inc.data_ptr(), use_log)
+            cess = capi.weight_cess(N, w.data_ptr(), inc.data_ptr(), use_log)
+            want_e = float(g[f"{name}_ess_{use_log}"])
+            want_c = float(g[f"{name}_cess_{use_log}"])
+            assert abs(ess - want_e) <= 1e-10 * abs(want_e), (name, use_log, ess, want_e)
+            assert abs(cess - want_c) <= 1e-10 * abs(want_c), (name, use_log, cess, want_c)

@@ -115,3 +115,43 @@ def test_reference_backends_agree():
     for r in rs:
         assert r["logz"] == ro["logz"]
         assert np.array_equal(r["mean_x"], ro["mean_x"])
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference harness not built")
+def test_prospective_golden_matches_reference():
+    """tests/golden/prospective.npz is what the vSMC build here gives."""
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "prospective.npz"))
+    rng = np.random.default_rng(77)
+    lw = rng.normal(size=7) * 2
+    inc = rng.normal(size=7)
+    assert np.array_equal(inc, g["small_inc"])
+    for use_log in (0, 1):
+        for cess in (0, 1):
+            key = f"small_{'cess' if cess else 'ess'}_{use_log}"
+            assert O.ref_weight_prospective(lw, inc, use_log, cess) == float(g[key])
+
+
+def test_resample_m_ne_n_golden():
+    """The C restatement's Resample(M, N) and cfrp_trans expansion against
+    vSMC's (tests/golden/resample_mn.npz)."""
+    import os
+
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_golden import MN_CASES
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "resample_mn.npz"))
+    n = 0
+    for M, N in MN_CASES:
+        w = g[f"M{M}_N{N}_w"]
+        for sch in range(6):
+            for seed, skip in ((103, 0), (7, 5)):
+                tag = f"M{M}_N{N}_s{sch}_{seed}_{skip}"
+                rep, cf, words = O.resample(sch, w, seed, skip, M=M, N=N)
+                assert np.array_equal(rep, g[tag + "_rep"]), tag
+                assert np.array_equal(cf, g[tag + "_cf"]), tag
+                assert words == int(g[tag + "_words"]), tag
+                n += 1
+    assert n == 12 * len(MN_CASES)

@@ -88,6 +88,13 @@ def lib():
     L.vsmc_cuda_resample.argtypes = [i32, u64, vp, vp, u64, C.POINTER(ThreefryState),
                                      vp, vp, vp, C.c_size_t, vp]
     L.vsmc_cuda_copy_f64.argtypes = [u64, C.c_uint32, vp, vp, vp, vp]
+    L.vsmc_cuda_resample_mn_workspace_size.restype = C.c_size_t
+    L.vsmc_cuda_resample_mn_workspace_size.argtypes = [u64, u64]
+    L.vsmc_cuda_resample_mn.argtypes = [i32, u64, u64, vp, vp, u64,
+                                        C.POINTER(ThreefryState), vp, vp, vp,
+                                        C.c_size_t, vp]
+    L.vsmc_cuda_weight_ess.argtypes = [u64, vp, vp, vp, i32, C.POINTER(f64), vp]
+    L.vsmc_cuda_weight_cess.argtypes = [u64, vp, vp, i32, C.POINTER(f64), vp]
     L.vsmc_cuda_resample_noalloc.argtypes = [i32, u64, vp, vp, u64,
                                              C.POINTER(ThreefryState), vp, vp, vp]
     L.vsmc_cuda_cv_config_default.argtypes = [C.POINTER(CVConfig)]
@@ -225,6 +232,37 @@ def resample(scheme, N, weight_ptr, rng: ThreefryState, rep_ptr, cf_ptr, ws_ptr,
                                    C.byref(rng), rep_ptr, cf_ptr, ws_ptr, ws_bytes, stream),
           "vsmc_cuda_resample")
     return int(rng.offset - before)
+
+
+def resample_mn_workspace_size(M, N) -> int:
+    return int(lib().vsmc_cuda_resample_mn_workspace_size(M, N))
+
+
+def resample_mn(scheme, M, N, weight_ptr, rng: ThreefryState, rep_ptr, cf_ptr, ws_ptr,
+                ws_bytes, uniforms_ptr=None, n_uniforms=0, stream=None) -> int:
+    """Resample(M, N) + cfrp_trans(M, N); returns the engine words drawn."""
+    before = rng.offset
+    check(lib().vsmc_cuda_resample_mn(scheme, M, N, weight_ptr, uniforms_ptr, n_uniforms,
+                                      C.byref(rng), rep_ptr, cf_ptr, ws_ptr, ws_bytes,
+                                      stream),
+          "vsmc_cuda_resample_mn")
+    return int(rng.offset - before)
+
+
+def weight_ess(N, lw_ptr, w_ptr, inc_ptr, use_log, stream=None) -> float:
+    """WeightSet::ess(inc, use_log) of device weights (see the C ABI)."""
+    v = C.c_double()
+    check(lib().vsmc_cuda_weight_ess(N, lw_ptr, w_ptr, inc_ptr, 1 if use_log else 0,
+                                     C.byref(v), stream), "vsmc_cuda_weight_ess")
+    return v.value
+
+
+def weight_cess(N, w_ptr, inc_ptr, use_log, stream=None) -> float:
+    """WeightSet::cess(inc, use_log) of device weights (see the C ABI)."""
+    v = C.c_double()
+    check(lib().vsmc_cuda_weight_cess(N, w_ptr, inc_ptr, 1 if use_log else 0,
+                                      C.byref(v), stream), "vsmc_cuda_weight_cess")
+    return v.value
 
 
 NOALLOC_MAX_N = 262144

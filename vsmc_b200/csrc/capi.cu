@@ -132,6 +132,48 @@ k_wadd_reduce(const LseAcc *tiles, int ntiles, WeightCtl *ctl)
     }
 }
 
+// Sums of prospective weights b_i for WeightSet::ess(first, use_log) and
+// cess(first, use_log) (core/weight_set.hpp:132-186, compute_ess :385-409,
+// compute_cess :411-431):
+//   kind 0 (ESS, use_log):  b = exp(lw + inc - max), online log-sum-exp;
+//   kind 1 (ESS, linear):   b = w * inc;           s1 = sum b, s2 = sum b^2;
+//   kind 2 (CESS, use_log): s1 = sum w e^inc,      s2 = sum w e^inc e^inc;
+//   kind 3 (CESS, linear):  s1 = sum w inc,        s2 = sum w inc inc.
+// ESS = s1^2 / s2 (the reference's 1 / sum (b / sum b)^2), CESS = s1^2 / s2
+// (above^2 / below).
+__global__ void __launch_bounds__(kThreads)
+k_prospective_tiles(long long N, const double *lw, const double *w,
+                    const double *inc, int kind, LseAcc *tiles)
+{
+    __shared__ LseAcc sh[kThreads / 32];
+    const long long base = (long long)blockIdx.x * kTile;
+    LseAcc acc;
+    acc.init();
+    if (kind != 0)
+        acc.m = 0.0; // plain sums: every partial has the same reference 0
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        const long long i = base + (long long)j * kThreads + threadIdx.x;
+        if (i >= N)
+            continue;
+        if (kind == 0) {
+            acc.add(__dadd_rn(lw[i], inc[i]), 0.0, 0.0);
+        } else if (kind == 1) {
+            const double b = __dmul_rn(w[i], inc[i]);
+            acc.s1 = __dadd_rn(acc.s1, b);
+            acc.s2 = __dadd_rn(acc.s2, __dmul_rn(b, b));
+        } else {
+            const double b = kind == 2 ? exp(inc[i]) : inc[i];
+            const double wb = __dmul_rn(w[i], b);
+            acc.s1 = __dadd_rn(acc.s1, wb);
+            acc.s2 = __dadd_rn(acc.s2, __dmul_rn(wb, b));
+        }
+    }
+    const LseAcc r = block_reduce_lse(acc, sh);
+    if (threadIdx.x == 0)
+        tiles[blockIdx.x] = r;
+}
+
 // lw += -max (normalize_log_weight); w = exp(lw) * (1 / sum).
 __global__ void k_wadd_apply(long long N, double *lw, double *w,
                              const WeightCtl *ctl)
@@ -276,6 +318,67 @@ int vsmc_cuda_weight_add_log(uint64_t N, double *lw, double *w,
     return VSMC_CUDA_OK;
 }
 
+namespace {
+
+int prospective(uint64_t N, const double *lw, const double *w,
+                const double *inc, int kind, double *out, void *stream,
+                const char *where)
+{
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int nt = (int)((N + kTile - 1) / kTile);
+    void *scratch = nullptr;
+    cudaError_t e = cudaMallocAsync(
+        &scratch, align256(sizeof(WeightCtl)) + sizeof(LseAcc) * nt, s);
+    if (e != cudaSuccess)
+        return cuda_status(e, where);
+    WeightCtl *ctl = static_cast<WeightCtl *>(scratch);
+    LseAcc *tiles = reinterpret_cast<LseAcc *>(
+        static_cast<char *>(scratch) + align256(sizeof(WeightCtl)));
+    k_prospective_tiles<<<nt, kThreads, 0, s>>>((long long)N, lw, w, inc,
+                                                kind, tiles);
+    k_wadd_reduce<<<1, kSpineThreads, 0, s>>>(tiles, nt, ctl);
+    WeightCtl h;
+    e = cudaMemcpyAsync(&h, ctl, sizeof(h), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(scratch, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+        return cuda_status(e, where);
+    *out = h.S1 * h.S1 / h.S2;
+    if (h.error || !(h.S2 > 0.0)) {
+        set_last_error(std::string(where) + ": degenerate weights");
+        *out = NAN;
+        return VSMC_CUDA_EDEGENERATE;
+    }
+    return VSMC_CUDA_OK;
+}
+
+} // namespace
+
+int vsmc_cuda_weight_ess(uint64_t N, const double *log_weight,
+                         const double *weight, const double *inc, int use_log,
+                         double *ess, void *stream)
+{
+    if (N == 0 || inc == nullptr || ess == nullptr ||
+        (use_log ? log_weight == nullptr : weight == nullptr)) {
+        set_last_error("vsmc_cuda_weight_ess: invalid arguments");
+        return VSMC_CUDA_EINVAL;
+    }
+    return prospective(N, log_weight, weight, inc, use_log ? 0 : 1, ess,
+                       stream, "vsmc_cuda_weight_ess");
+}
+
+int vsmc_cuda_weight_cess(uint64_t N, const double *weight, const double *inc,
+                          int use_log, double *cess, void *stream)
+{
+    if (N == 0 || weight == nullptr || inc == nullptr || cess == nullptr) {
+        set_last_error("vsmc_cuda_weight_cess: invalid arguments");
+        return VSMC_CUDA_EINVAL;
+    }
+    return prospective(N, nullptr, weight, inc, use_log ? 2 : 3, cess, stream,
+                       "vsmc_cuda_weight_cess");
+}
+
 size_t vsmc_cuda_resample_workspace_size(uint64_t N)
 {
     if (N == 0 || N > (1ull << 30))
@@ -332,6 +435,95 @@ int vsmc_cuda_resample(int scheme, uint64_t N, const double *weight,
         return cuda_status(e, "vsmc_cuda_resample");
     if (h.error != 0) {
         set_last_error("vsmc_cuda_resample: look-back wait gave up");
+        return h.error;
+    }
+    rng->offset = h.offset;
+    return VSMC_CUDA_OK;
+}
+
+size_t vsmc_cuda_resample_mn_workspace_size(uint64_t M, uint64_t N)
+{
+    if (M == 0 || M > (1ull << 30) || N > (1ull << 30))
+        return 0;
+    const long long Nmax = (long long)(M > N ? M : N);
+    return resample_workspace_bytes(Nmax) + 2 * align256((size_t)Nmax * 4);
+}
+
+int vsmc_cuda_resample_mn(int scheme, uint64_t M, uint64_t N,
+                          const double *weight, const double *uniforms,
+                          uint64_t n_uniforms, vsmc_cuda_threefry_state *rng,
+                          int32_t *replication, int32_t *copy_from,
+                          void *workspace, size_t workspace_bytes,
+                          void *stream)
+{
+    const size_t need = vsmc_cuda_resample_mn_workspace_size(M, N);
+    if (scheme < 0 || scheme > 5 || need == 0 || weight == nullptr ||
+        rng == nullptr || workspace == nullptr || workspace_bytes < need ||
+        (uniforms == nullptr && n_uniforms != 0) || n_uniforms > N ||
+        (reinterpret_cast<uintptr_t>(workspace) & 255) != 0) {
+        set_last_error("vsmc_cuda_resample_mn: invalid arguments (scheme, "
+                       "M >= 1, N, null pointer, or workspace too small / "
+                       "not 256-byte aligned)");
+        return VSMC_CUDA_EINVAL;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const bool sys = scheme == VSMC_CUDA_SYSTEMATIC ||
+                     scheme == VSMC_CUDA_RESIDUAL_SYSTEMATIC;
+    const long long Nmax = (long long)(M > N ? M : N);
+    char *wsp = static_cast<char *>(workspace);
+    int32_t *cf_scratch =
+        reinterpret_cast<int32_t *>(wsp + resample_workspace_bytes(Nmax));
+    int32_t *rep = replication != nullptr
+                       ? replication
+                       : cf_scratch + align256((size_t)Nmax * 4) / 4;
+    cudaError_t e = cudaSuccess;
+    if (N == 0) {
+        // inversion(M, 0, ...) leaves every count at zero; only the
+        // systematic sequence draws its one word, in its constructor
+        // (rng/u01.hpp:253-263)
+        e = cudaMemsetAsync(rep, 0, M * 4, s);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess)
+            return cuda_status(e, "vsmc_cuda_resample_mn");
+        rng->offset += sys ? 1 : 0;
+        return VSMC_CUDA_OK;
+    }
+    if (M == N)
+        return vsmc_cuda_resample(scheme, N, weight, uniforms, n_uniforms,
+                                  rng, replication, copy_from, workspace,
+                                  workspace_bytes, stream);
+    ResampleWorkspace ws = carve_workspace(workspace, Nmax);
+    ResampleCtl h;
+    std::memset(&h, 0, sizeof(h));
+    h.active = 1;
+    h.offset = rng->offset;
+    h.Nout = (long long)N;
+    e = cudaMemcpyAsync(ws.ctl, &h, sizeof(h), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_resample_mn: control block");
+    EngineRef eng;
+    for (int i = 0; i < 4; ++i) {
+        eng.key.v[i] = rng->key[i];
+        eng.ctr.v[i] = rng->ctr[i];
+    }
+    WeightsGiven w;
+    w.w = weight;
+    launch_resample_core(scheme, w, (long long)M, eng, ws, uniforms,
+                         (long long)n_uniforms, false, rep, cf_scratch, s,
+                         false, /*cfrp=*/false, (long long)N);
+    if (copy_from != nullptr)
+        launch_expand(rep, (long long)M, (long long)N, ws, copy_from, s);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_resample_mn: launch");
+    e = cudaMemcpyAsync(&h, ws.ctl, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_resample_mn");
+    if (h.error != 0) {
+        set_last_error("vsmc_cuda_resample_mn: replication did not sum to N");
         return h.error;
     }
     rng->offset = h.offset;

@@ -37,7 +37,17 @@ struct ResampleCtl {
     int kbits;            // bin index: K = 2^kbits bins over [0, 1)
     unsigned long long spec_offset; // engine offset the held speculative
                                     // sorted sequence was drawn at (~0: none)
+    long long Nout; // children in total when it differs from the number of
+                    // weights (Resample(M, N) with M != N); 0: the same
 };
+
+// The number of children of a resampling of N weights (ctl->Nout when the
+// caller asked for M != N).
+__device__ __forceinline__ long long resample_children(const ResampleCtl *ctl,
+                                                      long long N)
+{
+    return ctl->Nout > 0 ? ctl->Nout : N;
+}
 
 struct EngineRef {
     u64x4 key;
@@ -205,7 +215,7 @@ k_tile_sums_body(W wsrc, long long N, const ResampleCtl *ctl, double *tile_sum,
     long long *shk = sm.shk;
     wsrc.prepare();
     const long long base = (long long)bid * kTile;
-    const double Nd = (double)N;
+    const double Nd = (double)resample_children(ctl, N);
     double s = 0.0;
     long long ks = 0;
 #pragma unroll
@@ -332,7 +342,7 @@ k_spine_weights_body(const double *tile_sum, const long long *tile_k,
     double *shd = sm.shd;
     long long *shk = sm.shk;
     double &coeff_sh = sm.coeff;
-    long long NN = N;
+    long long NN = resample_children(ctl, N);
     double coeff = 1.0;
     if (Residual) {
         spine_scan_ll(tile_k, tile_kexcl, ntiles, shk);
@@ -349,7 +359,7 @@ k_spine_weights_body(const double *tile_sum, const long long *tile_k,
             coeff_sh = __ddiv_rn(1.0, total);
         __syncthreads();
         coeff = coeff_sh;
-        NN = N - tile_kexcl[ntiles];
+        NN = resample_children(ctl, N) - tile_kexcl[ntiles];
     }
     spine_scan_f64(tile_sum, tile_excl, ntiles, coeff, shd);
     if (threadIdx.x == 0) {
@@ -852,7 +862,8 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     const int tile = tile_bid;
     const long long base = (long long)tile * kTile;
     const long long NN = ctl->NN;
-    const double Nd = (double)N;
+    const long long Nout = resample_children(ctl, N);
+    const double Nd = (double)Nout;
     const double coeff_r = Residual ? ctl->coeff_r : 1.0;
     const double u0 = Sys ? ctl->u0 : 0.0;
     const double delta = ctl->delta;
@@ -1007,8 +1018,9 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     for (int j = 0; j < kItems; ++j) {
         const int i = i0 + j;
         kprefix += k_int[j];
-        // R_{<=i} = count_i + K_{<=i}; the last particle closes at N
-        const int R = (i >= iN - 1) ? iN : cnt[j] + kprefix;
+        // R_{<=i} = count_i + K_{<=i}; the last particle closes at the
+        // number of children
+        const int R = (i >= iN - 1) ? (int)Nout : cnt[j] + kprefix;
         if (rep[j] == 0) {
             cf[j] = -(zloc + 1);
             ++zloc;
@@ -1424,9 +1436,13 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
                                  const double *u_given, long long n_given,
                                  bool spine_done, int32_t *rep_out,
                                  int32_t *copy_from, cudaStream_t s,
-                                 bool sorted_ready = false)
+                                 bool sorted_ready = false, bool cfrp = true,
+                                 long long Nout = 0)
 {
     const int nt = resample_ntiles(N);
+    // uniforms: up to the number of children (Nout when it is not N)
+    const long long Nu = Nout > N ? Nout : N;
+    const int ntu_dev = resample_ntiles(Nu);
     const bool residual = scheme == VSMC_CUDA_RESIDUAL ||
                           scheme == VSMC_CUDA_RESIDUAL_STRATIFIED ||
                           scheme == VSMC_CUDA_RESIDUAL_SYSTEMATIC;
@@ -1458,7 +1474,7 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
                 ws.ctl);
     }
     const double *u = ws.u;
-    long long n_u = N;
+    long long n_u = Nu;
     if (u_given != nullptr) {
         const int ntu = (int)((n_given + kTile - 1) / kTile);
         if (n_given > 0) {
@@ -1470,18 +1486,18 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
         }
         n_u = n_given;
     } else if (strat) {
-        const long long blocks = N / 4 + 2;
+        const long long blocks = Nu / 4 + 2;
         k_uniforms_stratified<<<(unsigned)((blocks + kThreads - 1) / kThreads),
                                 kThreads, 0, s>>>(eng, ws.ctl, ws.u,
                                                   ws.bins);
     } else if (!sys && !sorted_ready) {
-        k_sorted_tile_sums<<<nt, kThreads, 0, s>>>(eng, ws.ctl,
-                                                   ws.u_tile_sum, ws.u);
+        k_sorted_tile_sums<<<ntu_dev, kThreads, 0, s>>>(eng, ws.ctl,
+                                                        ws.u_tile_sum, ws.u);
         k_sorted_spine<<<1, kSpineThreads, 0, s>>>(ws.u_tile_sum,
                                                    ws.u_tile_excl, ws.ctl);
-        k_sorted_uniforms<<<nt, kThreads, 0, s>>>(eng, ws.ctl,
-                                                  ws.u_tile_excl, ws.u,
-                                                  ws.bins);
+        k_sorted_uniforms<<<ntu_dev, kThreads, 0, s>>>(eng, ws.ctl,
+                                                       ws.u_tile_excl, ws.u,
+                                                       ws.bins);
     }
     const long long *kex = residual ? ws.tile_kexcl : nullptr;
 #define VSMC_INVERT(R, S)                                                     \
@@ -1497,12 +1513,99 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
     else
         VSMC_INVERT(false, false);
 #undef VSMC_INVERT
-    k_zero_spine<<<1, kSpineThreads, 0, s>>>(ws.tile_zeros, ws.tile_sinc_last,
-                                             ws.zexcl, ws.tfirst, ws.tlast,
-                                             nt, ws.ctl);
-    k_cfrp_fill<<<nt, kThreads, 0, s>>>(N, ws.ctl, ws.sinc, ws.zexcl,
-                                        ws.tfirst, ws.tlast, copy_from);
+    if (cfrp) {
+        k_zero_spine<<<1, kSpineThreads, 0, s>>>(
+            ws.tile_zeros, ws.tile_sinc_last, ws.zexcl, ws.tfirst, ws.tlast,
+            nt, ws.ctl);
+        k_cfrp_fill<<<nt, kThreads, 0, s>>>(N, ws.ctl, ws.sinc, ws.zexcl,
+                                            ws.tfirst, ws.tlast, copy_from);
+    }
     k_resample_done<<<1, 1, 0, s>>>(ws.ctl);
+}
+
+// internal::cfrp_trans for M != N (resample/common.hpp:110-117): parent i
+// fills the next rep[i] slots, so copy_from is the parents in order, each
+// repeated rep[i] times.  Per-tile sums of rep, their exclusive spine, the
+// inclusive prefix P of rep, then slot j takes the first parent with
+// P > j (a binary search per slot keeps a parent with many children from
+// serialising its tile).
+static __global__ void __launch_bounds__(kThreads)
+k_rep_tile_sums(const int32_t *rep, long long M, long long *tile_sum)
+{
+    __shared__ long long sh[kThreads / 32];
+    const long long base = (long long)blockIdx.x * kTile;
+    long long v = 0;
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        const long long i = base + (long long)j * kThreads + threadIdx.x;
+        if (i < M)
+            v += rep[i];
+    }
+    long long total;
+    block_excl_scan(v, sh, total);
+    if (threadIdx.x == 0)
+        tile_sum[blockIdx.x] = total;
+}
+
+static __global__ void __launch_bounds__(kSpineThreads)
+k_rep_spine(const long long *tile_sum, long long *tile_excl, int ntiles)
+{
+    __shared__ long long sh[kSpineThreads / 32];
+    spine_scan_ll(tile_sum, tile_excl, ntiles, sh);
+}
+
+static __global__ void __launch_bounds__(kThreads)
+k_rep_prefix(const int32_t *rep, long long M, const long long *tile_excl,
+             int32_t *incl)
+{
+    __shared__ long long sh[kThreads / 32];
+    const long long base = (long long)blockIdx.x * kTile;
+    const long long i0 = base + (long long)threadIdx.x * kItems;
+    long long r[kItems];
+    long long run = 0;
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        r[j] = i0 + j < M ? rep[i0 + j] : 0;
+        run += r[j];
+    }
+    long long total;
+    long long off = block_excl_scan(run, sh, total) + tile_excl[blockIdx.x];
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        off += r[j];
+        if (i0 + j < M)
+            incl[i0 + j] = (int32_t)off;
+    }
+}
+
+static __global__ void k_expand_fill(const int32_t *incl, long long M,
+                                     long long N, int32_t *copy_from)
+{
+    const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N)
+        return;
+    long long lo = 0, hi = M - 1; // incl[M - 1] == N > j
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (incl[mid] > j)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    copy_from[j] = (int32_t)lo;
+}
+
+// The launches of the M != N copy_from (4 kernels).
+inline void launch_expand(const int32_t *rep, long long M, long long N,
+                          ResampleWorkspace &ws, int32_t *copy_from,
+                          cudaStream_t s)
+{
+    const int nt = resample_ntiles(M);
+    k_rep_tile_sums<<<nt, kThreads, 0, s>>>(rep, M, ws.tile_k);
+    k_rep_spine<<<1, kSpineThreads, 0, s>>>(ws.tile_k, ws.tile_kexcl, nt);
+    k_rep_prefix<<<nt, kThreads, 0, s>>>(rep, M, ws.tile_kexcl, ws.sinc);
+    k_expand_fill<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(ws.sinc, M, N,
+                                                               copy_from);
 }
 
 // The speculative Multinomial sequence for the next resampling (see
