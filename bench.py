@@ -625,6 +625,30 @@ def main():
     e2e = replicas.job_throughput(world, N, K, e2e_s)
 
     extras = {}
+    if world > 1 and not args.no_extras:
+        # filter-partitioned batch: each rank runs its share of the 4096
+        # filters in one batch on its own GPU; no collective on the data
+        # path; the job's time is the slowest rank's
+        bN, bT, bobs = batched_workload(capi)
+        parts = replicas.partition_filters([int(n) * int(t) for n, t in zip(bN, bT)], world)
+        mine = parts[rank]
+        sub = (bN[mine], bT[mine], [bobs[k] for k in mine])
+        res = {}
+        for fname, fv in (("fp64", capi.FP64), ("mixed", capi.MIXED)):
+            barrier()
+            r = batched_run(capi, fv, *sub)
+            slow_ms = max_over_ranks(r["ms_per_run"])
+            res[fname] = {"filters_per_s": len(bN) / (slow_ms / 1e3),
+                          "particle_steps_per_s": float(np.sum(bN * bT)) / (slow_ms / 1e3),
+                          "ms_per_run": slow_ms, "rank0": r}
+        if rank == 0:
+            extras["batched"] = {
+                "workload": "4096 CV Student-t filters, N log-uniform [2^10, 2^16], T uniform "
+                            "[50, 500], Multinomial, threshold 0.5, seeds 101+k, streams k; "
+                            f"partitioned over {world} ranks by particle-steps (no collective "
+                            "on the data path), time = slowest rank",
+                "filters": len(bN), "particle_steps": int(np.sum(bN * bT)),
+                "filters_per_rank": [len(p) for p in parts], **res}
     if rank == 0 and world == 1 and not args.no_extras:
         if args.form == "fp64":
             extras["forms"] = forms_compare(capi, N, sch, K, W, ox, oy, sp, ms / K)

@@ -1,4 +1,8 @@
-"""Host side of the multi-GPU run: independent filter replicas, one per rank.
+"""Host side of the multi-GPU run: independent filters spread over ranks.
+
+Single filter: independent replicas, one per rank.  Batched filters: the
+filter list is partitioned across ranks (each rank runs its share in one
+batch on its own GPU), with no collective on the data path.
 
 One filter's SMC step does not shard without an exchange step, so the
 sharded unit is a whole filter.  Rank r runs its own filter of N particles
@@ -43,3 +47,43 @@ def job_throughput(world: int, N: int, steps: int, seconds: float) -> float:
     if seconds <= 0.0:
         raise ValueError("elapsed time must be positive")
     return world * N * steps / seconds
+
+
+def partition_filters(work, world: int) -> list:
+    """Filter indices of each rank for a batch whose filter k costs work[k]
+    (particles x steps): longest processing time first, each filter to the
+    rank with the least work so far (ties to the lower rank), then each
+    rank's list in ascending filter order.  Deterministic, so every rank
+    computes the same partition without a collective; every filter goes to
+    exactly one rank."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(work)), key=lambda k: (-int(work[k]), k))
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for k in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(k)
+        load[r] += int(work[k])
+    return [sorted(p) for p in parts]
+
+
+def gather_results(values, dist=None, device="cpu"):
+    """Every rank's list of per-filter results (equal-length float lists are
+    not required): all_gather of a padded tensor, returned as a list per
+    rank.  Used for the job's results, never on the timed data path."""
+    if dist is None:
+        return [list(values)]
+    import torch
+
+    world = dist.get_world_size()
+    n = torch.tensor([len(values)], dtype=torch.int64, device=device)
+    ns = [torch.zeros_like(n) for _ in range(world)]
+    dist.all_gather(ns, n)
+    m = int(max(int(x.item()) for x in ns))
+    t = torch.full((max(m, 1),), float("nan"), dtype=torch.float64, device=device)
+    if values:
+        t[: len(values)] = torch.tensor(list(values), dtype=torch.float64, device=device)
+    ts = [torch.zeros_like(t) for _ in range(world)]
+    dist.all_gather(ts, t)
+    return [ts[r][: int(ns[r].item())].tolist() for r in range(world)]
