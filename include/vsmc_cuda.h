@@ -152,7 +152,8 @@ size_t vsmc_cuda_resample_mn_workspace_size(uint64_t M, uint64_t N);
 
 /* Resample<Scheme>::operator()(M, N, rng, weight, replication) followed by
  * internal::cfrp_trans(M, N, replication, copy_from) for M weights and N
- * children (resample/*.hpp; common.hpp:57-118): replication has M entries
+ * children (include/vsmc/resample/multinomial.hpp to residual_systematic.hpp;
+ * common.hpp:57-118): replication has M entries
  * summing to N; copy_from (N entries, may be NULL) is, for M != N, the
  * cfrp_trans expansion (parent i repeated replication[i] times, in order)
  * and for M == N the same as vsmc_cuda_resample.  M >= 1; N = 0 leaves every
@@ -552,13 +553,28 @@ int vsmc_cuda_cv_batch_set_graphs(vsmc_cuda_cv_batch *b, int enable);
 int vsmc_cuda_cv_batch_set_launch_shape(vsmc_cuda_cv_batch *b,
                                         int move_blocks, int final_threads);
 
+/* Tiling of vsmc_cuda_cv_batch_run: filters of at most `block_tiles` tiles
+ * (2048 particles each; 0 <= block_tiles <= 64) run block-per-filter -- one
+ * persistent launch in which a CTA takes a filter and runs all of its
+ * remaining steps with block barriers only, beside the grid-per-filter
+ * steps of the larger filters on a second stream -- and the rest
+ * grid-per-filter (one launch per kernel per step over every filter's
+ * tiles).  0 (the default of a new batch) runs every filter grid-per-filter.
+ * The tiling changes no result: both run the same per-tile code in the same
+ * summation order. */
+int vsmc_cuda_cv_batch_set_tiling(vsmc_cuda_cv_batch *b, int block_tiles);
+int vsmc_cuda_cv_batch_tiling(vsmc_cuda_cv_batch *b, int *block_tiles);
+
 /* The batch's autotuner: times a few steps of a trial copy of (a sample
  * of at most 256 of) the listed filters, with zero observations, under each
  * launch shape (the move compiled for 2, 3 or 4 x 256 threads per SM; the finalize
  * CTA at 1024 or 256 threads when every filter has at most 256 tiles) and
- * keeps the fastest for later steps.  The shapes change no result, and the
- * trial touches none of the batch's filters.  Synchronises; reports the
- * choice (each pointer may be NULL). */
+ * keeps the fastest for later steps; then, at that shape, times whole trial
+ * runs under each tiling (block_tiles 0, 1, 2, 4, ... up to the largest
+ * trial filter; vsmc_cuda_cv_batch_set_tiling) and keeps the fastest.  The
+ * shapes and the tiling change no result, and the trial touches none of the
+ * batch's filters.  Synchronises; reports the launch shape (each pointer
+ * may be NULL; vsmc_cuda_cv_batch_tiling gives the tiling). */
 int vsmc_cuda_cv_batch_autotune(vsmc_cuda_cv_batch *b, uint32_t n,
                                 const uint32_t *slots, int *move_blocks,
                                 int *final_threads);

@@ -49,13 +49,18 @@ def assert_same(h, s, what):
         assert np.array_equal(h[k], s[k]), (what, k)
 
 
+@pytest.mark.parametrize("tiling", [0, 4, 64])
 @pytest.mark.parametrize("form", [0, 1])
 @pytest.mark.parametrize("scheme", range(6))
-def test_batch_run_equals_single(golden, capi, scheme, form):
+def test_batch_run_equals_single(golden, capi, scheme, form, tiling):
+    """Every slot equals the lone filter bit for bit whether it runs
+    grid-per-filter (tiling 0), block-per-filter (tiling 64: all of SPECS)
+    or either, by size (tiling 4: filters of at most 4 tiles block)."""
     obs = [series(capi, golden, k, T, sid) for k, (N, T, seed, sid) in enumerate(SPECS)]
     with capi.CVBatch(len(SPECS), scheme=scheme, form=form) as b:
         slots = [b.admit(N, T, seed, sid) for (N, T, seed, sid) in SPECS]
         b.set_observations(slots, obs)
+        b.set_tiling(tiling)
         b.run(slots)
         last = b.read_last(slots)
         hist = [b.history(s) for s in slots]
@@ -285,3 +290,45 @@ def test_batch_read_steps(golden, capi):
         s0 = b.admit(1000, 4)
         with pytest.raises(capi.VsmcCudaError):
             b.read_steps([s0], [1])  # no step taken yet
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_block_tiling_graph_and_rerun(golden, capi, graphs):
+    """Block-per-filter beside grid-per-filter in one run, recorded as a CUDA
+    graph (or launched directly), run twice after a re-initialise: both runs
+    equal the all-grid run."""
+    scheme = 0
+    obs = [series(capi, golden, k, T, sid) for k, (N, T, seed, sid) in enumerate(SPECS)]
+    res = {}
+    for tiling in (0, 2):
+        with capi.CVBatch(len(SPECS), scheme=scheme) as b:
+            b.set_graphs(graphs)
+            slots = [b.admit(N, T, seed, sid) for (N, T, seed, sid) in SPECS]
+            b.set_observations(slots, obs)
+            b.set_tiling(tiling)
+            assert b.tiling() == tiling
+            runs = []
+            for _ in range(2):
+                b.initialize(slots)
+                b.run(slots)
+                runs.append(([b.history(s) for s in slots],
+                             b.read_last(slots)["log_evidence"]))
+            res[tiling] = runs
+    for r in res[2] + res[0][1:]:
+        for k in range(len(SPECS)):
+            assert_same(r[0][k], res[0][0][0][k], k)
+        assert np.array_equal(r[1], res[0][0][1])
+
+
+def test_autotune_picks_a_tiling(golden, capi):
+    obs = [series(capi, golden, k, T, sid) for k, (N, T, seed, sid) in enumerate(SPECS)]
+    with capi.CVBatch(len(SPECS), scheme=3) as b:
+        slots = [b.admit(N, T, seed, sid) for (N, T, seed, sid) in SPECS]
+        b.set_observations(slots, obs)
+        b.autotune(slots)
+        assert b.tiling() in (0, 1, 2, 4, 8, 16, 32, 64)
+        b.run(slots)
+        hist = [b.history(s) for s in slots]
+    for k, (N, T, seed, sid) in enumerate(SPECS):
+        s = single(capi, N, T, 3, 0, seed, sid, *obs[k])
+        assert_same(hist[k], s, N)

@@ -142,6 +142,8 @@ def lib():
     L.vsmc_cuda_cv_batch_set_graphs.argtypes = [vp, i32]
     L.vsmc_cuda_cv_batch_set_launch_shape.argtypes = [vp, C.c_int, C.c_int]
     L.vsmc_cuda_cv_batch_read_steps.argtypes = [vp, u32, vp, vp, vp, vp, vp, vp]
+    L.vsmc_cuda_cv_batch_set_tiling.argtypes = [vp, C.c_int]
+    L.vsmc_cuda_cv_batch_tiling.argtypes = [vp, C.POINTER(C.c_int)]
     L.vsmc_cuda_cv_batch_autotune.argtypes = [vp, u32, vp, C.POINTER(C.c_int),
                                               C.POINTER(C.c_int)]
     L.vsmc_cuda_cv_server_create.argtypes = [C.POINTER(CVConfig), u32, u64, C.POINTER(vp)]
@@ -602,6 +604,16 @@ class CVBatch:
     def set_launch_shape(self, move_blocks, final_threads):
         check(lib().vsmc_cuda_cv_batch_set_launch_shape(self.h, move_blocks, final_threads),
               "vsmc_cuda_cv_batch_set_launch_shape")
+
+    def set_tiling(self, block_tiles):
+        """Filters of at most block_tiles tiles run block-per-filter."""
+        check(lib().vsmc_cuda_cv_batch_set_tiling(self.h, block_tiles),
+              "vsmc_cuda_cv_batch_set_tiling")
+
+    def tiling(self) -> int:
+        v = C.c_int()
+        check(lib().vsmc_cuda_cv_batch_tiling(self.h, C.byref(v)), "vsmc_cuda_cv_batch_tiling")
+        return v.value
 
     def autotune(self, slots):
         """Pick the launch shapes by timing a trial copy; returns

@@ -284,6 +284,257 @@ static __global__ void kb_step_done(BatchSlot *slots, const int32_t *work,
     b.t += 1;
 }
 
+// ---- block per filter ----------------------------------------------------
+// Small filters (a few tiles) spend most of a grid-per-filter step waiting
+// at kernel boundaries: each of the step's 9 launches has one or two CTAs
+// of work per filter.  kb_block_run gives each such filter one CTA that
+// runs all of the filter's remaining steps with block barriers only: the
+// same per-tile bodies in the same order (tile by tile where the grid runs
+// tiles in parallel), so every filter's results equal those of a lone
+// filter bit for bit.  The spines and the finalize run on the CTA's 256
+// threads, which gives the same sums as 1024 while a filter has at most
+// 256 tiles.  Persistent CTAs take filters from a queue, largest work
+// first.
+constexpr int kBlockMaxTiles = 64; // largest filter kb_block_run takes
+
+struct BlockItem {
+    int32_t slot;
+    int32_t steps;
+};
+
+template <bool Residual>
+union SmemBlockPhase {
+    SmemFinal fin;
+    SmemTileSums ts;
+    SmemSpine sp;
+    SmemNone none;
+    SmemSortedSums ss;
+    SmemSortedUniforms su;
+    SmemInvert<Residual> inv;
+    SmemZeroSpine zsp;
+    SmemFill fill;
+};
+
+template <bool Residual>
+struct SmemBlock {
+    double2 pts[2 * kTile]; // the move's polar points
+    SmemBlockPhase<Residual> ph;
+    double agg[kBlockMaxTiles];
+    double sh_w[2][7 * kMoveWarps];
+    int item;
+};
+
+template <bool Residual>
+constexpr size_t block_smem_bytes()
+{
+    return sizeof(SmemBlock<Residual>);
+}
+
+// Two CTAs per SM: the whole step in one kernel needs more registers than
+// the move alone (three CTAs spilled).
+constexpr int kBlockCtasPerSm = 2;
+
+template <typename Real, bool Residual, bool Sys, bool Strat>
+__global__ void __launch_bounds__(kThreads, kBlockCtasPerSm)
+kb_block_run(BatchSlot *slots, const BlockItem *items, int n, int *queue,
+             BatchConst c)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SmemBlock<Residual> &sm = *reinterpret_cast<SmemBlock<Residual> *>(smem_raw);
+    for (;;) {
+        if (threadIdx.x == 0)
+            sm.item = atomicAdd(queue, 1);
+        __syncthreads();
+        const int it = sm.item;
+        __syncthreads();
+        if (it >= n)
+            return;
+        BatchSlot &b = slots[items[it].slot];
+        const int steps = items[it].steps;
+        const int nt = b.ntiles;
+        for (int st = 0; st < steps; ++st) {
+            // move: kb_move's body, tile by tile
+            {
+                const MoveArgs<Real> a = batch_move_args<Real>(b, c.p);
+                int buf = 0;
+                if (a.iter == 0) {
+                    const MoveStep<Real> ms = move_step<Real, true>(a);
+                    for (int tile = 0; tile < nt; ++tile, buf ^= 1)
+                        cv_move_tile<Real, true>(a, ms, tile, sm.sh_w[buf],
+                                                 sm.pts);
+                } else {
+                    const MoveStep<Real> ms = move_step<Real, false>(a);
+                    for (int tile = 0; tile < nt; ++tile, buf ^= 1)
+                        cv_move_tile<Real, false>(a, ms, tile, sm.sh_w[buf],
+                                                  sm.pts);
+                }
+            }
+            __syncthreads();
+            // finalize: kb_finalize's body
+            {
+                FinalizeArgs a;
+                a.ctl = b.ctl;
+                a.ts = b.tile_stats;
+                a.ntiles = nt;
+                a.N = b.N;
+                a.threshold = c.threshold;
+                a.t = b.t;
+                a.init = b.t == 0;
+                a.anchored = c.anchored;
+                a.obs_x = b.obs_x;
+                a.obs_y = b.obs_y;
+                a.hist_ess = b.hist_ess;
+                a.hist_resampled = b.hist_resampled;
+                a.hist_logz_inc = b.hist_logz_inc;
+                a.hist_mean_x = b.hist_mean_x;
+                a.hist_mean_y = b.hist_mean_y;
+                a.rctl = b.rws.ctl;
+                a.tile_excl = b.rws.tile_excl;
+                a.residual = c.residual;
+                a.sys = c.sys;
+                a.eng = b.eng;
+                a.replay_flags = nullptr;
+                a.compare = 0;
+                k_cv_finalize_body(a, sm.agg, kBlockMaxTiles, sm.ph.fin);
+            }
+            __syncthreads();
+            const WeightsFromLog<Real> w = batch_weights<Real>(b);
+            if (Residual) {
+                for (int tile = 0; tile < nt; ++tile) {
+                    k_tile_sums_body<WeightsFromLog<Real>, true>(
+                        w, b.N, b.rws.ctl, b.rws.tile_sum, b.rws.tile_k,
+                        tile, sm.ph.ts);
+                    __syncthreads();
+                }
+                k_spine_weights_body<true, Sys>(
+                    b.rws.tile_sum, b.rws.tile_k, b.rws.tile_excl,
+                    b.rws.tile_kexcl, nt, b.N, b.eng, b.rws.ctl, 0, sm.ph.sp);
+                __syncthreads();
+            }
+            if (Strat) {
+                const long long blocks = b.N / 4 + 2;
+                for (long long g = 0; g < blocks; g += kThreads)
+                    k_uniforms_stratified_body(
+                        b.eng, b.rws.ctl, b.rws.u, b.rws.bins,
+                        (unsigned long long)(g + threadIdx.x), sm.ph.none);
+                __syncthreads();
+            } else if (!Sys) {
+                for (int tile = 0; tile < nt; ++tile) {
+                    k_sorted_tile_sums_body(b.eng, b.rws.ctl,
+                                            b.rws.u_tile_sum, b.rws.u, tile,
+                                            sm.ph.ss);
+                    __syncthreads();
+                }
+                k_sorted_spine_body(b.rws.u_tile_sum, b.rws.u_tile_excl,
+                                    b.rws.ctl, 0, sm.ph.sp);
+                __syncthreads();
+                for (int tile = 0; tile < nt; ++tile) {
+                    k_sorted_uniforms_body(b.eng, b.rws.ctl,
+                                           b.rws.u_tile_excl, b.rws.u,
+                                           b.rws.bins, tile, sm.ph.su);
+                    __syncthreads();
+                }
+            }
+            for (int tile = 0; tile < nt; ++tile) {
+                k_invert_body<WeightsFromLog<Real>, Residual, Sys>(
+                    w, b.N, b.rws.ctl, b.rws.tile_excl,
+                    Residual ? b.rws.tile_kexcl : nullptr, b.rws.u, b.N,
+                    b.rws.bins, nullptr, b.copy_from, b.rws.sinc,
+                    b.rws.tile_zeros, b.rws.tile_sinc_last, tile, sm.ph.inv);
+                __syncthreads();
+            }
+            k_zero_spine_body(b.rws.tile_zeros, b.rws.tile_sinc_last,
+                              b.rws.zexcl, b.rws.tfirst, b.rws.tlast, nt,
+                              b.rws.ctl, 0, sm.ph.zsp);
+            __syncthreads();
+            for (int tile = 0; tile < nt; ++tile) {
+                k_cfrp_fill_body(b.N, b.rws.ctl, b.rws.sinc, b.rws.zexcl,
+                                 b.rws.tfirst, b.rws.tlast, b.copy_from, tile,
+                                 sm.ph.fill);
+                __syncthreads();
+            }
+            // kb_step_done
+            if (threadIdx.x == 0) {
+                ResampleCtl *rc = b.rws.ctl;
+                if (rc->active)
+                    rc->offset += rc->words;
+                b.t += 1;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// The kb_block_run instance of a scheme and form: dynamic shared memory
+// above the default (set once at batch creation) and its launch.
+template <typename Real, bool R, bool Sy, bool St>
+cudaError_t block_smem_one()
+{
+    return cudaFuncSetAttribute(kb_block_run<Real, R, Sy, St>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)block_smem_bytes<R>());
+}
+
+template <typename Real>
+cudaError_t block_smem_real(int scheme)
+{
+    switch (scheme) {
+    case VSMC_CUDA_MULTINOMIAL:
+        return block_smem_one<Real, false, false, false>();
+    case VSMC_CUDA_RESIDUAL:
+        return block_smem_one<Real, true, false, false>();
+    case VSMC_CUDA_STRATIFIED:
+        return block_smem_one<Real, false, false, true>();
+    case VSMC_CUDA_SYSTEMATIC:
+        return block_smem_one<Real, false, true, false>();
+    case VSMC_CUDA_RESIDUAL_STRATIFIED:
+        return block_smem_one<Real, true, false, true>();
+    default:
+        return block_smem_one<Real, true, true, false>();
+    }
+}
+
+inline cudaError_t set_block_smem(int scheme, int form)
+{
+    return form == VSMC_CUDA_MIXED ? block_smem_real<float>(scheme)
+                                   : block_smem_real<double>(scheme);
+}
+
+template <typename Real>
+void launch_block_real(int scheme, BatchSlot *slots, const BlockItem *items,
+                       int n, int *queue, const BatchConst &c, int grid,
+                       cudaStream_t s)
+{
+    const size_t sm_res = block_smem_bytes<true>();
+    const size_t sm_plain = block_smem_bytes<false>();
+    switch (scheme) {
+    case VSMC_CUDA_MULTINOMIAL:
+        kb_block_run<Real, false, false, false>
+            <<<grid, kThreads, sm_plain, s>>>(slots, items, n, queue, c);
+        break;
+    case VSMC_CUDA_RESIDUAL:
+        kb_block_run<Real, true, false, false>
+            <<<grid, kThreads, sm_res, s>>>(slots, items, n, queue, c);
+        break;
+    case VSMC_CUDA_STRATIFIED:
+        kb_block_run<Real, false, false, true>
+            <<<grid, kThreads, sm_plain, s>>>(slots, items, n, queue, c);
+        break;
+    case VSMC_CUDA_SYSTEMATIC:
+        kb_block_run<Real, false, true, false>
+            <<<grid, kThreads, sm_plain, s>>>(slots, items, n, queue, c);
+        break;
+    case VSMC_CUDA_RESIDUAL_STRATIFIED:
+        kb_block_run<Real, true, false, true>
+            <<<grid, kThreads, sm_res, s>>>(slots, items, n, queue, c);
+        break;
+    default:
+        kb_block_run<Real, true, true, false>
+            <<<grid, kThreads, sm_res, s>>>(slots, items, n, queue, c);
+        break;
+    }
+}
+
 // Fresh filter state (Sampler::initialize's reset): step count 0, cleared
 // control block; the resample engine position is kept.
 __device__ __forceinline__ void reset_slot(BatchSlot &b)
@@ -480,6 +731,18 @@ struct vsmc_cuda_cv_batch {
     int tune_move;        // x 256 threads per SM the move is compiled for: 2, 3, 4
     int tune_final;       // finalize CTA size: 256 or 1024
     int max_ntiles;       // largest slot admitted, in tiles
+    // tiling (vsmc_cuda_cv_batch_autotune): filters of at most tune_block
+    // tiles run block-per-filter in kb_block_run (0: every filter runs
+    // grid-per-filter); no result depends on it
+    int tune_block;
+    int sms;                  // multiprocessors of the device
+    BlockItem *d_items;       // capacity block-per-filter work items
+    BlockItem *h_items;       // pinned staging
+    int *d_queue;             // kb_block_run's work counter
+    cudaEvent_t items_staged; // the last copy out of h_items is done
+    cudaStream_t block_stream;     // block-per-filter launches
+    cudaStream_t block_cap_stream; // their capture twin
+    cudaEvent_t ev_fork, ev_join;
 };
 
 namespace {
@@ -707,6 +970,55 @@ void launch_run_steps(vsmc_cuda_cv_batch *b, const std::vector<int> &active,
         launch_step_any(b, a, tile0[a], s);
 }
 
+// The block-per-filter part of a run: `bs` forks from `s`, resets the work
+// counter and runs one persistent kb_block_run over the staged items; the
+// grid-per-filter steps go on `s` meanwhile; join_block_part joins them.
+void launch_block_part(vsmc_cuda_cv_batch *b, int nitems, cudaStream_t s,
+                       cudaStream_t bs)
+{
+    cudaEventRecord(b->ev_fork, s);
+    cudaStreamWaitEvent(bs, b->ev_fork, 0);
+    cudaMemsetAsync(b->d_queue, 0, sizeof(int), bs);
+    const int grid = std::min(nitems, kBlockCtasPerSm * b->sms);
+    if (b->model.form == VSMC_CUDA_MIXED)
+        launch_block_real<float>(b->model.scheme, b->d_slots, b->d_items,
+                                 nitems, b->d_queue, b->bc, grid, bs);
+    else
+        launch_block_real<double>(b->model.scheme, b->d_slots, b->d_items,
+                                  nitems, b->d_queue, b->bc, grid, bs);
+    b->launches += 1;
+}
+
+void join_block_part(vsmc_cuda_cv_batch *b, cudaStream_t s, cudaStream_t bs)
+{
+    cudaEventRecord(b->ev_join, bs);
+    cudaStreamWaitEvent(s, b->ev_join, 0);
+}
+
+// Items of the block-per-filter part (slot, remaining steps), the largest
+// work first, copied to the device on the batch's stream.
+int stage_block_items(vsmc_cuda_cv_batch *b, const std::vector<uint32_t> &sm)
+{
+    cudaError_t e = cudaEventSynchronize(b->items_staged);
+    if (e != cudaSuccess)
+        return cuda_status(e, "vsmc_cuda_cv_batch: block staging");
+    std::vector<uint32_t> o(sm);
+    std::stable_sort(o.begin(), o.end(), [b](uint32_t a, uint32_t c) {
+        const double wa = (double)b->slots[a].N * (double)(b->T_obs[a] - b->t[a]);
+        const double wc = (double)b->slots[c].N * (double)(b->T_obs[c] - b->t[c]);
+        return wa > wc;
+    });
+    for (size_t k = 0; k < o.size(); ++k)
+        b->h_items[k] = BlockItem{(int32_t)o[k],
+                                  (int32_t)(b->T_obs[o[k]] - b->t[o[k]])};
+    e = cudaMemcpyAsync(b->d_items, b->h_items, o.size() * sizeof(BlockItem),
+                        cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaEventRecord(b->items_staged, b->stream);
+    return e == cudaSuccess ? VSMC_CUDA_OK
+                            : cuda_status(e, "vsmc_cuda_cv_batch: block items");
+}
+
 int check_slots(const vsmc_cuda_cv_batch *b, uint32_t n,
                 const uint32_t *slots, const char *what)
 {
@@ -822,6 +1134,16 @@ int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
     b->tune_move = 4;
     b->tune_final = 256;
     b->max_ntiles = 0;
+    b->tune_block = 0;
+    b->sms = 148;
+    b->d_items = nullptr;
+    b->h_items = nullptr;
+    b->d_queue = nullptr;
+    b->items_staged = nullptr;
+    b->block_stream = nullptr;
+    b->block_cap_stream = nullptr;
+    b->ev_fork = nullptr;
+    b->ev_join = nullptr;
     b->run_exec = nullptr;
     b->run_map = nullptr;
     b->run_launches = 0;
@@ -876,6 +1198,28 @@ int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
         e = cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming);
     if (e == cudaSuccess)
         e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->d_items, n * sizeof(BlockItem) + 256);
+    if (e == cudaSuccess) {
+        b->d_queue = reinterpret_cast<int *>(b->d_items + n); // after items
+        e = cudaMallocHost(&b->h_items, n * sizeof(BlockItem));
+    }
+    if (e == cudaSuccess)
+        e = cudaEventCreateWithFlags(&b->items_staged, cudaEventDisableTiming);
+    if (e == cudaSuccess)
+        e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess)
+        e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&b->block_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&b->block_cap_stream,
+                                      cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount,
+                                   dev);
+    if (e == cudaSuccess)
+        e = set_block_smem(model->scheme, model->form);
     if (e != cudaSuccess) {
         cudaGetLastError();
         set_last_error("vsmc_cuda_cv_batch_create: allocation failed");
@@ -887,6 +1231,8 @@ int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
     e = cudaMemsetAsync(b->d_slots, 0, n * sizeof(BatchSlot), b->stream);
     if (e == cudaSuccess)
         e = cudaEventRecord(b->staged, b->stream);
+    if (e == cudaSuccess)
+        e = cudaEventRecord(b->items_staged, b->stream);
     if (e != cudaSuccess) {
         vsmc_cuda_cv_batch_destroy(b);
         return cuda_status(e, "vsmc_cuda_cv_batch_create");
@@ -923,6 +1269,20 @@ int vsmc_cuda_cv_batch_destroy(vsmc_cuda_cv_batch *b)
     drop_run_graph(b);
     if (b->cap_stream != nullptr)
         cudaStreamDestroy(b->cap_stream);
+    if (b->block_stream != nullptr) {
+        cudaStreamSynchronize(b->block_stream);
+        cudaStreamDestroy(b->block_stream);
+    }
+    if (b->block_cap_stream != nullptr)
+        cudaStreamDestroy(b->block_cap_stream);
+    cudaFree(b->d_items);
+    cudaFreeHost(b->h_items);
+    if (b->items_staged != nullptr)
+        cudaEventDestroy(b->items_staged);
+    if (b->ev_fork != nullptr)
+        cudaEventDestroy(b->ev_fork);
+    if (b->ev_join != nullptr)
+        cudaEventDestroy(b->ev_join);
     cudaMemPoolDestroy(b->pool);
     cudaError_t e = cudaGetLastError();
     delete b;
@@ -1202,21 +1562,35 @@ int vsmc_cuda_cv_batch_run(vsmc_cuda_cv_batch *b, uint32_t n,
         return st;
     if (n == 0)
         return VSMC_CUDA_OK;
-    // longest remaining series first: the slots still running at step k
-    // are a prefix of the list, and so are their tiles
-    std::vector<uint32_t> w(slots, slots + n);
+    // small filters (at most tune_block tiles) run block-per-filter, the
+    // rest grid-per-filter, longest remaining series first: the slots still
+    // running at step k are a prefix of the list, and so are their tiles
+    std::vector<uint32_t> all(slots, slots + n), w, small;
+    for (uint32_t x : all) {
+        if (b->tune_block > 0 && b->slots[x].ntiles <= b->tune_block &&
+            b->T_obs[x] > b->t[x])
+            small.push_back(x);
+        else
+            w.push_back(x);
+    }
     std::stable_sort(w.begin(), w.end(), [b](uint32_t a, uint32_t c) {
         return b->T_obs[a] - b->t[a] > b->T_obs[c] - b->t[c];
     });
+    const uint32_t nw = (uint32_t)w.size();
+    if (!small.empty()) {
+        st = stage_block_items(b, small);
+        if (st != VSMC_CUDA_OK)
+            return st;
+    }
     long long tiles = 0;
     st = stage_work(b, w, &tiles);
     if (st != VSMC_CUDA_OK)
         return st;
-    std::vector<long long> tile0(n + 1, 0);
-    for (uint32_t k = 0; k < n; ++k)
+    std::vector<long long> tile0(nw + 1, 0);
+    for (uint32_t k = 0; k < nw; ++k)
         tile0[k + 1] = tile0[k] + b->slots[w[k]].ntiles;
     std::vector<int> active;
-    int a = (int)n;
+    int a = (int)nw;
     for (uint64_t step = 0;; ++step) {
         while (a > 0 && b->T_obs[w[a - 1]] - b->t[w[a - 1]] <= step)
             --a;
@@ -1224,16 +1598,22 @@ int vsmc_cuda_cv_batch_run(vsmc_cuda_cv_batch *b, uint32_t n,
             break;
         active.push_back(a);
     }
+    const int nsmall = (int)small.size();
     cudaError_t e = cudaSuccess;
-    if (b->use_graphs && !active.empty()) {
-        // the whole run as one CUDA graph, reused while the work list and
-        // its step counts repeat (kernels read everything else from the
-        // slot records)
+    if (b->use_graphs && (!active.empty() || nsmall > 0)) {
+        // the whole run as one CUDA graph, reused while the work lists and
+        // their step counts repeat (kernels read everything else from the
+        // slot records and the staged block items)
         std::vector<uint64_t> key;
-        key.reserve(2 * n);
-        for (uint32_t k = 0; k < n; ++k) {
+        key.reserve(2 * n + 2);
+        for (uint32_t k = 0; k < nw; ++k) {
             key.push_back(w[k]);
             key.push_back(b->T_obs[w[k]] - b->t[w[k]]);
+        }
+        key.push_back(~0ull);
+        for (uint32_t x : small) {
+            key.push_back(x);
+            key.push_back(b->T_obs[x] - b->t[x]);
         }
         if (b->run_exec == nullptr || key != b->run_key ||
             b->run_map != b->d_map) {
@@ -1243,7 +1623,12 @@ int vsmc_cuda_cv_batch_run(vsmc_cuda_cv_batch *b, uint32_t n,
                                        cudaStreamCaptureModeThreadLocal);
             if (e == cudaSuccess) {
                 const uint64_t before = b->launches;
+                if (nsmall > 0)
+                    launch_block_part(b, nsmall, b->cap_stream,
+                                      b->block_cap_stream);
                 launch_run_steps(b, active, tile0, b->cap_stream);
+                if (nsmall > 0)
+                    join_block_part(b, b->cap_stream, b->block_cap_stream);
                 b->run_launches = b->launches - before;
                 e = cudaStreamEndCapture(b->cap_stream, &g);
             }
@@ -1262,7 +1647,11 @@ int vsmc_cuda_cv_batch_run(vsmc_cuda_cv_batch *b, uint32_t n,
         e = cudaGraphLaunch(b->run_exec, b->stream);
         b->launches += b->run_launches;
     } else {
+        if (nsmall > 0)
+            launch_block_part(b, nsmall, b->stream, b->block_stream);
         launch_run_steps(b, active, tile0, b->stream);
+        if (nsmall > 0)
+            join_block_part(b, b->stream, b->block_stream);
     }
     for (uint32_t k = 0; k < n; ++k)
         b->t[slots[k]] = b->T_obs[slots[k]];
@@ -1506,6 +1895,28 @@ int vsmc_cuda_cv_batch_set_launch_shape(vsmc_cuda_cv_batch *b,
     return VSMC_CUDA_OK;
 }
 
+int vsmc_cuda_cv_batch_set_tiling(vsmc_cuda_cv_batch *b, int block_tiles)
+{
+    if (b == nullptr || block_tiles < 0 || block_tiles > kBlockMaxTiles) {
+        set_last_error("vsmc_cuda_cv_batch_set_tiling: block_tiles must be "
+                       "0.." + std::to_string(kBlockMaxTiles));
+        return VSMC_CUDA_EINVAL;
+    }
+    if (block_tiles != b->tune_block) {
+        drop_run_graph(b); // recorded with the old tiling
+        b->tune_block = block_tiles;
+    }
+    return VSMC_CUDA_OK;
+}
+
+int vsmc_cuda_cv_batch_tiling(vsmc_cuda_cv_batch *b, int *block_tiles)
+{
+    if (b == nullptr || block_tiles == nullptr)
+        return VSMC_CUDA_EINVAL;
+    *block_tiles = b->tune_block;
+    return VSMC_CUDA_OK;
+}
+
 int vsmc_cuda_cv_batch_autotune(vsmc_cuda_cv_batch *b, uint32_t n,
                                 const uint32_t *slots, int *move_blocks,
                                 int *final_threads)
@@ -1577,6 +1988,35 @@ int vsmc_cuda_cv_batch_autotune(vsmc_cuda_cv_batch *b, uint32_t n,
                 best_final = finals[jf];
             }
         }
+    // tiling: whole trial runs (kTrialT steps) with the filters of at most
+    // K tiles block-per-filter, K = 0 (all grid-per-filter) and powers of
+    // two up to the largest trial filter
+    int best_block = b->tune_block;
+    if (st == VSMC_CUDA_OK) {
+        t->tune_move = best_move;
+        t->tune_final = best_final;
+        best_ms = 1e30f;
+        for (int K = 0; K <= kBlockMaxTiles && st == VSMC_CUDA_OK;
+             K = K == 0 ? 1 : 2 * K) {
+            if (K > 1 && K / 2 >= t->max_ntiles)
+                break; // every trial filter ran block-per-filter already
+            t->tune_block = K;
+            float ms = 0.0f;
+            for (int rep = 0; rep < 2 && st == VSMC_CUDA_OK; ++rep) {
+                st = vsmc_cuda_cv_batch_initialize(t, m, ts.data());
+                cudaEventRecord(e0, b->stream);
+                if (st == VSMC_CUDA_OK)
+                    st = vsmc_cuda_cv_batch_run(t, m, ts.data());
+                cudaEventRecord(e1, b->stream);
+                cudaEventSynchronize(e1);
+                cudaEventElapsedTime(&ms, e0, e1); // the second, warm run
+            }
+            if (st == VSMC_CUDA_OK && ms < best_ms) {
+                best_ms = ms;
+                best_block = K;
+            }
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->launches += t->launches;
@@ -1586,6 +2026,8 @@ int vsmc_cuda_cv_batch_autotune(vsmc_cuda_cv_batch *b, uint32_t n,
     if (st != VSMC_CUDA_OK)
         return st;
     st = vsmc_cuda_cv_batch_set_launch_shape(b, best_move, best_final);
+    if (st == VSMC_CUDA_OK)
+        st = vsmc_cuda_cv_batch_set_tiling(b, best_block);
     if (st != VSMC_CUDA_OK)
         return st;
     if (move_blocks)
