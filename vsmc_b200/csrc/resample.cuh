@@ -1168,14 +1168,18 @@ k_zero_spine_body(const int32_t *tile_zeros, const int32_t *tile_sinc_last,
     }
 }
 
+// The zero-slot spine, then the engine position (the words the inversion
+// counted are final here; nothing after this kernel reads the offset).
 static __global__ void __launch_bounds__(kSpineThreads)
 k_zero_spine(const int32_t *tile_zeros, const int32_t *tile_sinc_last,
              int32_t *zexcl, int32_t *tfirst, int32_t *tlast, int ntiles,
-             const ResampleCtl *ctl)
+             ResampleCtl *ctl)
 {
     __shared__ SmemZeroSpine sm;
     k_zero_spine_body(tile_zeros, tile_sinc_last, zexcl, tfirst, tlast, ntiles,
         ctl, blockIdx.x, sm);
+    if (threadIdx.x == 0 && ctl->active)
+        ctl->offset += ctl->words;
 }
 
 // internal::cfrp_trans for the slots without offspring (common.hpp:94-106):
@@ -1415,7 +1419,7 @@ inline int resample_launches(int scheme, bool parity)
                      scheme == VSMC_CUDA_RESIDUAL_SYSTEMATIC;
     const bool strat = scheme == VSMC_CUDA_STRATIFIED ||
                        scheme == VSMC_CUDA_RESIDUAL_STRATIFIED;
-    int n = 4; // invert, zero spine, cfrp fill, done
+    int n = 3; // invert, zero spine (and engine position), cfrp fill
     if (residual)
         n += 2;
     if (parity)
@@ -1514,13 +1518,15 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
         VSMC_INVERT(false, false);
 #undef VSMC_INVERT
     if (cfrp) {
+        // the spine kernel also advances the engine position
         k_zero_spine<<<1, kSpineThreads, 0, s>>>(
             ws.tile_zeros, ws.tile_sinc_last, ws.zexcl, ws.tfirst, ws.tlast,
             nt, ws.ctl);
         k_cfrp_fill<<<nt, kThreads, 0, s>>>(N, ws.ctl, ws.sinc, ws.zexcl,
                                             ws.tfirst, ws.tlast, copy_from);
+    } else {
+        k_resample_done<<<1, 1, 0, s>>>(ws.ctl);
     }
-    k_resample_done<<<1, 1, 0, s>>>(ws.ctl);
 }
 
 // internal::cfrp_trans for M != N (resample/common.hpp:110-117): parent i
