@@ -345,7 +345,12 @@ int prospective(uint64_t N, const double *lw, const double *w,
     if (e != cudaSuccess)
         return cuda_status(e, where);
     *out = h.S1 * h.S1 / h.S2;
-    if (h.error || !(h.S2 > 0.0)) {
+    // the log form needs a finite maximum and a positive sum; the plain
+    // forms only finite sums (increments may be negative) and S2 > 0
+    const bool bad = kind == 0 ? h.error != 0
+                               : !(h.S1 == h.S1 && h.S1 > -INFINITY &&
+                                   h.S1 < INFINITY && h.S2 < INFINITY);
+    if (bad || !(h.S2 > 0.0)) {
         set_last_error(std::string(where) + ": degenerate weights");
         *out = NAN;
         return VSMC_CUDA_EDEGENERATE;

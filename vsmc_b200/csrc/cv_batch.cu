@@ -1091,21 +1091,12 @@ int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
     if (b == nullptr)
         return VSMC_CUDA_ENOMEM;
     b->model = *model;
-    {
-        const int sm = (int)kPolarSmemBytes;
-        cudaFuncSetAttribute(kb_move<double, 2>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-        cudaFuncSetAttribute(kb_move<double, 3>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-        cudaFuncSetAttribute(kb_move<double, 4>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-        cudaFuncSetAttribute(kb_move<float, 2>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-        cudaFuncSetAttribute(kb_move<float, 3>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-        cudaFuncSetAttribute(kb_move<float, 4>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    }
+    set_move_smem_attribute(kb_move<double, 2>);
+    set_move_smem_attribute(kb_move<double, 3>);
+    set_move_smem_attribute(kb_move<double, 4>);
+    set_move_smem_attribute(kb_move<float, 2>);
+    set_move_smem_attribute(kb_move<float, 3>);
+    set_move_smem_attribute(kb_move<float, 4>);
     b->bc.p = cv_param(*model);
     b->bc.threshold = model->threshold;
     b->bc.residual = is_residual(model->scheme);

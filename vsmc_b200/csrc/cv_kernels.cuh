@@ -411,21 +411,30 @@ k_cv_move(MoveArgs<Real> a)
 }
 
 // The move kernels take kPolarSmemBytes of dynamic shared memory (above
-// the 48 KiB default); set once per device before their first launch.
+// the 48 KiB default) and prefer the shared-memory carve-out that fits
+// three such CTAs per SM; set once per device before their first launch.
+template <typename K>
+inline cudaError_t set_move_smem_attribute(K kernel)
+{
+    cudaError_t e = cudaFuncSetAttribute(
+        kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (int)kPolarSmemBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kernel,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+    return e;
+}
+
 inline cudaError_t set_move_smem_attributes()
 {
-    const int b = (int)kPolarSmemBytes;
-    cudaError_t e = cudaFuncSetAttribute(
-        k_cv_move<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    cudaError_t e = set_move_smem_attribute(k_cv_move<double, true>);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_cv_move<double, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        e = set_move_smem_attribute(k_cv_move<double, false>);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_cv_move<float, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        e = set_move_smem_attribute(k_cv_move<float, true>);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_cv_move<float, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        e = set_move_smem_attribute(k_cv_move<float, false>);
     return e;
 }
 
