@@ -321,3 +321,44 @@ def test_prospective_ess_cess(capi):
             want_c = float(g[f"{name}_cess_{use_log}"])
             assert abs(ess - want_e) <= 1e-10 * abs(want_e), (name, use_log, ess, want_e)
             assert abs(cess - want_c) <= 1e-10 * abs(want_c), (name, use_log, cess, want_c)
+
+
+@pytest.mark.parametrize("sch", range(6))
+def test_benchmark_size_bit_exact(capi, sch):
+    """At 2^24 particles (the benchmark size) with random weights, the device
+    resampler equals the oracle's restatement of the reference (sequential
+    `accw += w[i]`, resample/common.hpp:76-79) exactly: replication,
+    copy_from and engine words."""
+    N = 1 << 24
+    rng = np.random.default_rng(2024 + sch)
+    lw = rng.normal(size=N) * 2.0
+    w = np.exp(lw - lw.max())
+    w /= w.sum()
+    ref_rep, ref_cf, ref_words, uni = O.resample(sch, w, 103, 7, want_uniforms=True)
+    rep, cf, words = gpu_resample(capi, sch, w, 103, 7,
+                                  uni if sch in LOG_EXP_SCHEMES else None)
+    assert words == ref_words
+    assert np.array_equal(rep, ref_rep)
+    assert np.array_equal(cf, ref_cf)
+
+
+@pytest.mark.parametrize("sch", [0, 2, 3])
+def test_tie_heavy_weights_bit_exact(capi, sch):
+    """Weights whose every addition to the running sum is a rounding tie
+    (0.5 followed by 2^-54 steps: the sequential sum stays at 0.5 by
+    round-half-even while the exact sum grows), so every tile holds more
+    special elements than it keeps and is summed element by element; with
+    runs of ordinary weights between them.  Equal to the oracle bit for
+    bit."""
+    N = (1 << 18) + 123
+    rng = np.random.default_rng(sch)
+    w = rng.uniform(0.5, 1.5, size=N) * (0.5 / N)
+    w[: N // 3] = 2.0 ** -54
+    w[0] = 0.5
+    w[N // 3: N // 3 + 5000] = 2.0 ** -60
+    ref_rep, ref_cf, ref_words, uni = O.resample(sch, w, 77, 0, want_uniforms=True)
+    rep, cf, words = gpu_resample(capi, sch, w, 77, 0,
+                                  uni if sch in LOG_EXP_SCHEMES else None)
+    assert words == ref_words
+    assert np.array_equal(rep, ref_rep)
+    assert np.array_equal(cf, ref_cf)

@@ -136,10 +136,10 @@ k_wadd_reduce(const LseAcc *tiles, int ntiles, WeightCtl *ctl)
 // cess(first, use_log) (core/weight_set.hpp:132-186, compute_ess :385-409,
 // compute_cess :411-431):
 //   kind 0 (ESS, use_log):  b = exp(lw + inc - max), online log-sum-exp;
-//   kind 1 (ESS, linear):   b = w * inc;           s1 = sum b, s2 = sum b^2;
+//   kind 1 (ESS, linear):   b = w * inc;           s1 = sum |b|, s2 = sum b^2;
 //   kind 2 (CESS, use_log): s1 = sum w e^inc,      s2 = sum w e^inc e^inc;
 //   kind 3 (CESS, linear):  s1 = sum w inc,        s2 = sum w inc inc.
-// ESS = s1^2 / s2 (the reference's 1 / sum (b / sum b)^2), CESS = s1^2 / s2
+// ESS = s1^2 / s2 (the reference's 1 / sum (b / asum b)^2), CESS = s1^2 / s2
 // (above^2 / below).
 __global__ void __launch_bounds__(kThreads)
 k_prospective_tiles(long long N, const double *lw, const double *w,
@@ -159,8 +159,9 @@ k_prospective_tiles(long long N, const double *lw, const double *w,
         if (kind == 0) {
             acc.add(__dadd_rn(lw[i], inc[i]), 0.0, 0.0);
         } else if (kind == 1) {
+            // the reference normalises by asum, a sum of |b|
             const double b = __dmul_rn(w[i], inc[i]);
-            acc.s1 = __dadd_rn(acc.s1, b);
+            acc.s1 = __dadd_rn(acc.s1, fabs(b));
             acc.s2 = __dadd_rn(acc.s2, __dmul_rn(b, b));
         } else {
             const double b = kind == 2 ? exp(inc[i]) : inc[i];

@@ -247,7 +247,30 @@ kb_invert(const BatchSlot *slots, const TileRef *map)
         batch_weights<Real>(b), b.N, b.rws.ctl, b.rws.tile_excl,
         Residual ? b.rws.tile_kexcl : nullptr, b.rws.u, b.N, b.rws.bins,
         nullptr, b.copy_from, b.rws.sinc, b.rws.tile_zeros,
-        b.rws.tile_sinc_last, r.tile, sm);
+        b.rws.tile_sinc_last, b.rws.ex, r.tile, sm);
+}
+
+// The exact cumulative weight (exact_scan.cuh): per tile, then per slot.
+template <typename Real, bool Residual, bool Raw = false>
+__global__ void __launch_bounds__(kThreads)
+kb_exact_tiles(const BatchSlot *slots, const TileRef *map)
+{
+    __shared__ SmemExactTiles sm;
+    const TileRef r = map[blockIdx.x];
+    const BatchSlot &b = slots[r.slot];
+    k_exact_tiles_body<WeightsFromLog<Real>, Residual, Raw>(
+        batch_weights<Real>(b), b.N, b.rws.ctl, b.rws.tile_excl, b.rws.ex,
+        r.tile, sm);
+}
+
+template <typename Real, bool Residual, bool Raw = false>
+__global__ void __launch_bounds__(kSpineThreads)
+kb_exact_spine(const BatchSlot *slots, const int32_t *work)
+{
+    __shared__ SmemExactSpine sm;
+    const BatchSlot &b = slots[work[blockIdx.x]];
+    k_exact_spine_body<WeightsFromLog<Real>, Residual, Raw>(
+        batch_weights<Real>(b), b.N, b.rws.ctl, b.ntiles, b.rws.ex, sm);
 }
 
 static __global__ void __launch_bounds__(kSpineThreads)
@@ -313,6 +336,8 @@ union SmemBlockPhase {
     SmemInvert<Residual> inv;
     SmemZeroSpine zsp;
     SmemFill fill;
+    SmemExactTiles ext;
+    SmemExactSpine exs;
 };
 
 template <bool Residual>
@@ -435,12 +460,33 @@ kb_block_run(BatchSlot *slots, const BlockItem *items, int n, int *queue,
                     __syncthreads();
                 }
             }
+            if (Residual) { // the residuals' exact sum and coefficient
+                for (int tile = 0; tile < nt; ++tile) {
+                    k_exact_tiles_body<WeightsFromLog<Real>, true, true>(
+                        w, b.N, b.rws.ctl, b.rws.tile_excl, b.rws.ex, tile,
+                        sm.ph.ext);
+                    __syncthreads();
+                }
+                k_exact_spine_body<WeightsFromLog<Real>, true, true>(
+                    w, b.N, b.rws.ctl, nt, b.rws.ex, sm.ph.exs);
+                __syncthreads();
+            }
+            for (int tile = 0; tile < nt; ++tile) {
+                k_exact_tiles_body<WeightsFromLog<Real>, Residual>(
+                    w, b.N, b.rws.ctl, b.rws.tile_excl, b.rws.ex, tile,
+                    sm.ph.ext);
+                __syncthreads();
+            }
+            k_exact_spine_body<WeightsFromLog<Real>, Residual>(
+                w, b.N, b.rws.ctl, nt, b.rws.ex, sm.ph.exs);
+            __syncthreads();
             for (int tile = 0; tile < nt; ++tile) {
                 k_invert_body<WeightsFromLog<Real>, Residual, Sys>(
                     w, b.N, b.rws.ctl, b.rws.tile_excl,
                     Residual ? b.rws.tile_kexcl : nullptr, b.rws.u, b.N,
                     b.rws.bins, nullptr, b.copy_from, b.rws.sinc,
-                    b.rws.tile_zeros, b.rws.tile_sinc_last, tile, sm.ph.inv);
+                    b.rws.tile_zeros, b.rws.tile_sinc_last, b.rws.ex, tile,
+                    sm.ph.inv);
                 __syncthreads();
             }
             k_zero_spine_body(b.rws.tile_zeros, b.rws.tile_sinc_last,
@@ -928,6 +974,18 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
         kb_sorted_uniforms<<<nt, kThreads, 0, s>>>(sl, map);
         launches += 3;
     }
+    if (residual) {
+        kb_exact_tiles<Real, true, true><<<nt, kThreads, 0, s>>>(sl, map);
+        kb_exact_spine<Real, true, true><<<n, kSpineThreads, 0, s>>>(sl,
+                                                                    work);
+        kb_exact_tiles<Real, true><<<nt, kThreads, 0, s>>>(sl, map);
+        kb_exact_spine<Real, true><<<n, kSpineThreads, 0, s>>>(sl, work);
+        launches += 2;
+    } else {
+        kb_exact_tiles<Real, false><<<nt, kThreads, 0, s>>>(sl, map);
+        kb_exact_spine<Real, false><<<n, kSpineThreads, 0, s>>>(sl, work);
+    }
+    launches += 2;
     if (residual && sys)
         kb_invert<Real, true, true><<<nt, kThreads, 0, s>>>(sl, map);
     else if (residual)

@@ -20,6 +20,7 @@
 #pragma once
 
 #include "smc_common.cuh"
+#include "exact_scan.cuh"
 
 namespace vsmc_b200 {
 
@@ -156,6 +157,19 @@ WeightsFromLog<float>::operator()(long long i) const
                      coeff);
 }
 
+// Relative error margin of the approximate cumulative weights the exact
+// scan classifies with (its spine comes from the weights' tile sums): FP64
+// weights carry a few ulps; weights of a float form differ from the move's
+// per-tile sums by the float rounding of lw - max (about 1e-6 relative).
+template <typename W>
+struct ExactMargin {
+    static constexpr double rel = 0x1p-44;
+};
+template <>
+struct ExactMargin<WeightsFromLog<float> > {
+    static constexpr double rel = 0x1p-19;
+};
+
 // Residual split of a weight: r = modf(N w, &k) (residual.hpp:61-62).
 __device__ __forceinline__ double residual_split(double w, double Nd,
                                                  double &k)
@@ -200,6 +214,10 @@ struct SmemInvert {
     double shd[kThreads / 32];
     long long bound[2];
     long long last[kThreads / 32];
+    // the tile's specials of the exact cumulative weight (exact_scan.cuh)
+    double sv[kExactCap];
+    unsigned long long kb[kExactCap];
+    SmemExactThread et;
 };
 
 // ---------------------------------------------------------------------------
@@ -834,6 +852,259 @@ __device__ __forceinline__ long long sys_count(double C, double u0,
 
 constexpr int kUStage = kTile; // uniforms staged in shared memory per tile
 
+// The weight the inversion scans for element i: w_i, or for the residual
+// schemes its residual r_i * coeff_r (residual.hpp:59-66).
+template <typename W, bool Residual>
+__device__ __forceinline__ double scan_weight(const W &wsrc, long long i,
+                                              double Nd, double coeff_r,
+                                              double *kint)
+{
+    double w = wsrc(i), k = 0.0;
+    if (Residual)
+        w = __dmul_rn(residual_split(w, Nd, k), coeff_r);
+    if (kint)
+        *kint = k;
+    return w;
+}
+
+struct SmemExactTiles {
+    double sw[kTile];
+    double shd[kThreads / 32];
+    SmemExactThread et;
+};
+
+// Phase A of the exact cumulative weight (exact_scan.cuh) for one tile.
+// Raw (residual schemes): the unscaled residuals, whose exact sum is the
+// reference's asum (residual.hpp:63) and so its coefficient.
+template <typename W, bool Residual, bool Raw = false>
+__device__ __forceinline__ void
+k_exact_tiles_body(W wsrc, long long N, const ResampleCtl *ctl,
+                   const double *tile_excl, ExactScan ex, int tile,
+                   SmemExactTiles &sm)
+{
+    // residual schemes without residual children scan nothing
+    if (!ctl->active || (Residual && ctl->NN <= 0))
+        return;
+    wsrc.prepare();
+    const long long base = (long long)tile * kTile;
+    const double Nd = (double)resample_children(ctl, N);
+    const double coeff_r = Residual && !Raw ? ctl->coeff_r : 1.0;
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        const int l = j * kThreads + threadIdx.x;
+        const long long i = base + l;
+        sm.sw[l] = i < N ? scan_weight<W, Residual>(wsrc, i, Nd, coeff_r,
+                                                    nullptr)
+                         : 0.0;
+    }
+    __syncthreads();
+    double w[kItems];
+    double run = 0.0;
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        w[j] = sm.sw[threadIdx.x * kItems + j];
+        run += w[j];
+    }
+    double total;
+    const double pre = block_excl_scan(run, sm.shd, total);
+    const long long i0 = base + (long long)threadIdx.x * kItems;
+    // the approximate spine is of the scaled weights; unscaled for Raw
+    const double a_apx = Raw ? __ddiv_rn(tile_excl[tile], ctl->coeff_r)
+                             : tile_excl[tile];
+    ExactThread x;
+    exact_thread(i0, N, w, a_apx, pre, ExactMargin<W>::rel, x, sm.et);
+    exact_tile_record(x, w, base, i0, N, tile, ex);
+}
+
+template <typename W, bool Residual, bool Raw = false>
+__global__ void __launch_bounds__(kThreads)
+k_exact_tiles(W wsrc, long long N, const ResampleCtl *ctl,
+              const double *tile_excl, ExactScan ex)
+{
+    __shared__ SmemExactTiles sm;
+    k_exact_tiles_body<W, Residual, Raw>(wsrc, N, ctl, tile_excl, ex,
+                                         blockIdx.x, sm);
+}
+
+constexpr int kExactDirtyStage = 256; // tiles with specials the spine stages
+
+struct SmemExactSpine {
+    unsigned long long shk[kSpineThreads / 32];
+    int shi[kSpineThreads / 32];
+    int nd;
+    // the walk's inputs, staged (when at most kExactDirtyStage tiles have
+    // specials and their specials fit kExactStage): for the q-th such tile
+    // d, its record, pk[d], pk of the clean run before it and that run's
+    // binade, and its specials at st[st_off[q]...]
+    ExactSpecial st[kExactStage];
+    int st_off[kExactDirtyStage];
+    int dq[kExactDirtyStage];
+    ExactTile tq[kExactDirtyStage];
+    unsigned long long run_k[kExactDirtyStage];
+    int run_e[kExactDirtyStage];
+};
+
+// Phase B (one CTA): the exact S before every tile and at every special.
+// Raw: the sum of the unscaled residuals sets coeff_r = 1 / sum, as the
+// reference's `1 / math::asum(M, rptr)` (residual.hpp:63).
+template <typename W, bool Residual, bool Raw = false>
+__device__ __forceinline__ void
+k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
+                   ExactScan ex, SmemExactSpine &sm)
+{
+    if (!ctl->active || (Residual && ctl->NN <= 0))
+        return;
+    wsrc.prepare();
+    const int bd = (int)blockDim.x;
+    // prefix of the clean tiles' k (tiles with specials count 0); its
+    // differences are taken in unsigned arithmetic, exact within a run
+    {
+        const int per = (nt + bd - 1) / bd;
+        const int b = threadIdx.x * per, e = min(b + per, nt);
+        unsigned long long run = 0;
+        int nd = 0;
+        for (int t = b; t < e; ++t) {
+            const ExactTile et = ex.tiles[t];
+            run += et.nspec == 0 ? et.k_total : 0ull;
+            nd += et.nspec != 0;
+        }
+        unsigned long long tot;
+        unsigned long long off = block_excl_scan(run, sm.shk, tot);
+        int ndt;
+        int doff = block_excl_scan(nd, sm.shi, ndt);
+        for (int t = b; t < e; ++t) {
+            const ExactTile et = ex.tiles[t];
+            ex.pk[t] = off;
+            off += et.nspec == 0 ? et.k_total : 0ull;
+            if (et.nspec != 0)
+                ex.dirty[doff++] = t;
+        }
+        if (threadIdx.x == bd - 1)
+            ex.pk[nt] = off;
+        if (threadIdx.x == 0)
+            sm.nd = ndt;
+    }
+    __syncthreads();
+    const int nd = sm.nd;
+    // stage the walk's inputs, one tile with specials per thread
+    const bool staged = nd <= kExactDirtyStage;
+    int nsq = 0;
+    if (staged && (int)threadIdx.x < nd) {
+        const int q = threadIdx.x;
+        const int d = ex.dirty[q];
+        const int prev = q > 0 ? ex.dirty[q - 1] : -1;
+        const ExactTile et = ex.tiles[d];
+        sm.dq[q] = d;
+        sm.tq[q] = et;
+        const bool run = d > prev + 1;
+        sm.run_k[q] = run ? ex.pk[d] - ex.pk[prev + 1] : 0ull;
+        sm.run_e[q] = run ? ex.tiles[prev + 1].e_last : kNoBinade;
+        nsq = et.nspec <= kExactCap ? et.nspec : 0;
+    }
+    int nst;
+    const int soff = block_excl_scan(nsq, sm.shi, nst);
+    const bool fits = staged && nst <= kExactStage;
+    if (fits && (int)threadIdx.x < nd)
+        sm.st_off[threadIdx.x] = soff;
+    __syncthreads();
+    if (fits) {
+        for (int q = 0; q < nd; ++q) {
+            const int ns = sm.tq[q].nspec;
+            if (ns > kExactCap)
+                continue;
+            for (int r = threadIdx.x; r < ns; r += bd)
+                sm.st[sm.st_off[q] + r] =
+                    ex.spec[(size_t)sm.dq[q] * kExactCap + r];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double Nd = (double)resample_children(ctl, N);
+        const double coeff_r = Residual && !Raw ? ctl->coeff_r : 1.0;
+        double S = 0.0;
+        int prev = -1;
+        for (int q = 0; q < nd; ++q) {
+            const int d = staged ? sm.dq[q] : ex.dirty[q];
+            const ExactTile et = staged ? sm.tq[q] : ex.tiles[d];
+            unsigned long long K = 0;
+            int ke = kNoBinade;
+            if (staged) {
+                K = sm.run_k[q];
+                ke = sm.run_e[q];
+            } else if (d > prev + 1) {
+                K = ex.pk[d] - ex.pk[prev + 1];
+                ke = ex.tiles[prev + 1].e_last;
+            }
+            if (K != 0) // the clean tiles prev + 1 .. d - 1
+                S = __dadd_rn(S, __dmul_rn((double)K, exact_pow2(ke - 52)));
+            ex.start[d] = S;
+            if (et.nspec <= kExactCap) {
+                unsigned long long kb = 0;
+                for (int r = 0; r < et.nspec; ++r) {
+                    const ExactSpecial sp =
+                        fits ? sm.st[sm.st_off[q] + r]
+                             : ex.spec[(size_t)d * kExactCap + r];
+                    const unsigned long long seg = sp.k_before - kb;
+                    if (seg != 0)
+                        S = __dadd_rn(S, __dmul_rn((double)seg,
+                                                   exact_pow2(sp.e_seg - 52)));
+                    S = __dadd_rn(S, sp.w);
+                    ex.s_spec[(size_t)d * kExactCap + r] = S;
+                    kb = sp.k_before;
+                }
+                const unsigned long long tail = et.k_total - kb;
+                if (tail != 0)
+                    S = __dadd_rn(S, __dmul_rn((double)tail,
+                                               exact_pow2(et.e_last - 52)));
+            } else {
+                // more specials than kept: the reference's loop itself
+                const long long b0 = (long long)d * kTile;
+                const long long b1 = min(b0 + (long long)kTile, N);
+                for (long long i = b0; i < b1; ++i) {
+                    S = __dadd_rn(S, scan_weight<W, Residual>(
+                                         wsrc, i, Nd, coeff_r, nullptr));
+                    ex.full[i] = S;
+                }
+            }
+            ex.s_out[d] = S;
+            prev = d;
+        }
+    }
+    __syncthreads();
+    // every clean tile and the end: the last tile with specials before it
+    // (tile 0 always has one: its first element) plus the exact run sum
+    for (int t = threadIdx.x; t <= nt; t += bd) {
+        if (t < nt && ex.tiles[t].nspec != 0)
+            continue;
+        int lo = 0, hi = nd - 1; // last q with dirty[q] < t
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (ex.dirty[mid] < t)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const int d = ex.dirty[lo];
+        const unsigned long long K = ex.pk[t] - ex.pk[d + 1];
+        double S = ex.s_out[d];
+        if (K != 0)
+            S = __dadd_rn(S, __dmul_rn((double)K,
+                                       exact_pow2(ex.tiles[d + 1].e_last -
+                                                  52)));
+        ex.start[t] = S;
+        if (Raw && t == nt)
+            ctl->coeff_r = __ddiv_rn(1.0, S);
+    }
+}
+
+template <typename W, bool Residual, bool Raw = false>
+__global__ void __launch_bounds__(kSpineThreads)
+k_exact_spine(W wsrc, long long N, ResampleCtl *ctl, int nt, ExactScan ex)
+{
+    __shared__ SmemExactSpine sm;
+    k_exact_spine_body<W, Residual, Raw>(wsrc, N, ctl, nt, ex, sm);
+}
+
 // The inversion kernel (internal::inversion, common.hpp:57-84, on the FP64
 // scan of the weights) and the first half of internal::cfrp_trans.
 // Residual: weights are r * coeff_r and k = floor(N w) is added back
@@ -847,7 +1118,7 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
               const long long *tile_kexcl, const double *u, long long n_u,
               const int32_t *L, int32_t *rep_out, int32_t *copy_from,
               int32_t *sinc_local, int32_t *tile_zeros, int32_t *tile_sinc_last,
-              int tile_bid, SmemInvert<Residual> &sm)
+              ExactScan ex, int tile_bid, SmemInvert<Residual> &sm)
 {
     if (!ctl->active)
         return;
@@ -868,8 +1139,14 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     const double u0 = Sys ? ctl->u0 : 0.0;
     const double delta = ctl->delta;
     const long long nu = Sys ? NN : min(NN, n_u);
-    const double a = tile_excl[tile];
-    const double b = tile_excl[tile + 1];
+    // the reference's cumulative weight before and at the end of the tile,
+    // exactly (exact_scan.cuh); the approximate spine classifies.  Residual
+    // schemes without residual children draw no uniform and scan nothing.
+    const bool exact = !(Residual && NN <= 0);
+    const double a = exact ? ex.start[tile] : 0.0;
+    const double b = exact ? ex.start[tile + 1] : 0.0;
+    const double a_apx = tile_excl[tile];
+    const int nsp_tile = exact ? ex.tiles[tile].nspec : 0;
 
     // uniforms that can fall in this tile: (ub(a), ub(b)], each found in a
     // bin window of about 8 values by one warp while the others load weights
@@ -906,6 +1183,11 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
         if (Residual)
             sk[l] = k;
     }
+    if (nsp_tile <= kExactCap && (int)threadIdx.x < nsp_tile) {
+        const size_t q = (size_t)tile * kExactCap + threadIdx.x;
+        sm.sv[threadIdx.x] = ex.s_spec[q];
+        sm.kb[threadIdx.x] = ex.spec[q].k_before;
+    }
     __syncthreads();
     // the tile's uniforms are loaded into registers now and written to
     // shared memory after the scan, so their latency overlaps the scan
@@ -928,7 +1210,19 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
         run += wv[j];
     }
     double total;
-    double pre = block_excl_scan(run, shd, total); // ends with a barrier
+    const double pre = block_excl_scan(run, shd, total); // ends with a barrier
+    // each particle's cumulative weight, exactly the reference's
+    double Cx[kItems];
+#pragma unroll
+    for (int j = 0; j < kItems; ++j)
+        Cx[j] = 0.0;
+    if (exact) {
+        ExactThread x;
+        exact_thread(base + (long long)threadIdx.x * kItems, N, wv, a_apx, pre,
+                     ExactMargin<W>::rel, x, sm.et);
+        exact_values(x, base + (long long)threadIdx.x * kItems, a, sm.sv,
+                     sm.kb, nsp_tile > kExactCap, ex.full, N, Cx);
+    }
     if (staged) {
 #pragma unroll
         for (int j = 0; j < kUStage / kThreads; ++j) {
@@ -951,10 +1245,7 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
         const int i = i0 + j;
-        pre += wv[j];
-        double C = fmin(__dadd_rn(a, pre), b);
-        if (i == (int)base + kTile - 1 || i == iN - 1)
-            C = b;
+        const double C = Cx[j];
         int c;
         if (i >= iN - 1) {
             c = iNN; // the last particle takes every remaining uniform
@@ -1065,7 +1356,7 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
 }
 
 #ifndef VSMC_INVERT_MIN_BLOCKS
-#define VSMC_INVERT_MIN_BLOCKS 5
+#define VSMC_INVERT_MIN_BLOCKS 4
 #endif
 
 template <typename W, bool Residual, bool Sys>
@@ -1073,11 +1364,12 @@ __global__ void __launch_bounds__(kThreads, VSMC_INVERT_MIN_BLOCKS)
 k_invert(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
          const long long *tile_kexcl, const double *u, long long n_u,
          const int32_t *L, int32_t *rep_out, int32_t *copy_from,
-         int32_t *sinc_local, int32_t *tile_zeros, int32_t *tile_sinc_last)
+         int32_t *sinc_local, int32_t *tile_zeros, int32_t *tile_sinc_last,
+         ExactScan ex)
 {
     __shared__ SmemInvert<Residual> sm;
     k_invert_body<W, Residual, Sys>(wsrc, N, ctl, tile_excl, tile_kexcl, u, n_u,
-        L, rep_out, copy_from, sinc_local, tile_zeros, tile_sinc_last,
+        L, rep_out, copy_from, sinc_local, tile_zeros, tile_sinc_last, ex,
         blockIdx.x, sm);
 }
 
@@ -1353,6 +1645,7 @@ struct ResampleWorkspace {
     int32_t *bins;         // N / 8 + 2 (bin index of the U01 sequence)
     double *u;             // N
     int32_t *sinc;         // N (tile-local surplus counts)
+    ExactScan ex;          // the exact cumulative weight (exact_scan.cuh)
 };
 
 constexpr int resample_ntiles(long long N)
@@ -1364,12 +1657,23 @@ constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
 // Bytes carve_workspace lays out for N particles (constexpr so that a static
 // scratch array can be sized from it at compile time).
+// Bytes of the exact scan's arrays for N particles.
+constexpr size_t exact_scan_bytes(long long N)
+{
+    const size_t nt = (size_t)resample_ntiles(N) + 1;
+    return align256(nt * sizeof(ExactTile)) +
+           align256(nt * kExactCap * sizeof(ExactSpecial)) +
+           align256(nt * kExactCap * 8) + 3 * align256(nt * 8) +
+           align256((size_t)N * 8) + align256(nt * 4);
+}
+
 constexpr size_t resample_workspace_bytes(long long N)
 {
     const size_t nt = (size_t)resample_ntiles(N) + 1;
     return align256(sizeof(ResampleCtl)) + 6 * align256(nt * 8) +
            5 * align256(nt * 4) + align256(((size_t)N / 8 + 2) * 4) +
-           align256((size_t)N * 8) + align256((size_t)N * 4);
+           align256((size_t)N * 8) + align256((size_t)N * 4) +
+           exact_scan_bytes(N);
 }
 
 inline ResampleWorkspace carve_workspace(void *base, long long N)
@@ -1406,6 +1710,22 @@ inline ResampleWorkspace carve_workspace(void *base, long long N)
     w.u = reinterpret_cast<double *>(p);
     p += align256((size_t)N * 8);
     w.sinc = reinterpret_cast<int32_t *>(p);
+    p += align256((size_t)N * 4);
+    w.ex.tiles = reinterpret_cast<ExactTile *>(p);
+    p += align256(nt * sizeof(ExactTile));
+    w.ex.spec = reinterpret_cast<ExactSpecial *>(p);
+    p += align256(nt * kExactCap * sizeof(ExactSpecial));
+    w.ex.s_spec = reinterpret_cast<double *>(p);
+    p += align256(nt * kExactCap * 8);
+    w.ex.start = reinterpret_cast<double *>(p);
+    p += align256(nt * 8);
+    w.ex.s_out = reinterpret_cast<double *>(p);
+    p += align256(nt * 8);
+    w.ex.pk = reinterpret_cast<unsigned long long *>(p);
+    p += align256(nt * 8);
+    w.ex.full = reinterpret_cast<double *>(p);
+    p += align256((size_t)N * 8);
+    w.ex.dirty = reinterpret_cast<int32_t *>(p);
     return w;
 }
 
@@ -1419,9 +1739,10 @@ inline int resample_launches(int scheme, bool parity)
                      scheme == VSMC_CUDA_RESIDUAL_SYSTEMATIC;
     const bool strat = scheme == VSMC_CUDA_STRATIFIED ||
                        scheme == VSMC_CUDA_RESIDUAL_STRATIFIED;
-    int n = 3; // invert, zero spine (and engine position), cfrp fill
+    int n = 5; // exact tiles and spine, invert, zero spine (and engine
+               // position), cfrp fill
     if (residual)
-        n += 2;
+        n += 4; // tile sums, spine, the residuals' exact sum
     if (parity)
         n += 2;
     else if (strat)
@@ -1504,10 +1825,28 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
                                                        ws.bins);
     }
     const long long *kex = residual ? ws.tile_kexcl : nullptr;
+    // the reference's sequential cumulative weight, exactly (for the
+    // residual schemes first the sum of the residuals, whose reciprocal
+    // scales them)
+    if (residual) {
+        k_exact_tiles<W, true, true><<<nt, kThreads, 0, s>>>(
+            wsrc, N, ws.ctl, ws.tile_excl, ws.ex);
+        k_exact_spine<W, true, true><<<1, kSpineThreads, 0, s>>>(
+            wsrc, N, ws.ctl, nt, ws.ex);
+        k_exact_tiles<W, true><<<nt, kThreads, 0, s>>>(wsrc, N, ws.ctl,
+                                                       ws.tile_excl, ws.ex);
+        k_exact_spine<W, true><<<1, kSpineThreads, 0, s>>>(wsrc, N, ws.ctl,
+                                                           nt, ws.ex);
+    } else {
+        k_exact_tiles<W, false><<<nt, kThreads, 0, s>>>(wsrc, N, ws.ctl,
+                                                        ws.tile_excl, ws.ex);
+        k_exact_spine<W, false><<<1, kSpineThreads, 0, s>>>(wsrc, N, ws.ctl,
+                                                            nt, ws.ex);
+    }
 #define VSMC_INVERT(R, S)                                                     \
     k_invert<W, R, S><<<nt, kThreads, 0, s>>>(                                \
         wsrc, N, ws.ctl, ws.tile_excl, kex, u, n_u, ws.bins, rep_out,        \
-        copy_from, ws.sinc, ws.tile_zeros, ws.tile_sinc_last)
+        copy_from, ws.sinc, ws.tile_zeros, ws.tile_sinc_last, ws.ex)
     if (residual && sys)
         VSMC_INVERT(true, true);
     else if (residual)
