@@ -176,7 +176,7 @@ int vsmc_cuda_resample_mn(int scheme, uint64_t M, uint64_t N,
  * host owns every allocation): the same kernels and results, with the
  * workspace (and the copy_from scratch when copy_from is NULL) taken from a
  * static device array the library holds for N <= VSMC_CUDA_NOALLOC_MAX_N
- * particles (about 4.1 MiB on every device that loads the library, kept
+ * particles (about 7.4 MiB on every device that loads the library, kept
  * until exit).  Larger N returns VSMC_CUDA_EINVAL.  It calls no cudaMalloc
  * or cudaFree.  The first call on each device looks up the array's device
  * address (cudaGetSymbolAddress, with that device current) and caches it

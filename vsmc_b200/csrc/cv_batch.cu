@@ -88,13 +88,17 @@ __device__ __forceinline__ MoveArgs<Real> batch_move_args(const BatchSlot &b,
     return a;
 }
 
+// A slot's weights; `normed`: with the exact normalisation coefficient of
+// the FP64 form (after its normalisation pass).
 template <typename Real>
 __device__ __forceinline__ WeightsFromLog<Real> batch_weights(
-    const BatchSlot &b)
+    const BatchSlot &b, bool normed = true)
 {
     WeightsFromLog<Real> w;
     w.lw = static_cast<const Real *>(b.lw);
     w.stats = &b.ctl->lw_max;
+    if (normed)
+        w = with_exact_coeff(w, &b.rws.ctl->coeff_w);
     return w;
 }
 
@@ -255,12 +259,12 @@ template <typename Real, bool Residual, bool Raw = false>
 __global__ void __launch_bounds__(kThreads)
 kb_exact_tiles(const BatchSlot *slots, const TileRef *map)
 {
-    __shared__ SmemExactTiles sm;
+    __shared__ SmemExactTiles<Residual> sm;
     const TileRef r = map[blockIdx.x];
     const BatchSlot &b = slots[r.slot];
     k_exact_tiles_body<WeightsFromLog<Real>, Residual, Raw>(
-        batch_weights<Real>(b), b.N, b.rws.ctl, b.rws.tile_excl, b.rws.ex,
-        r.tile, sm);
+        batch_weights<Real>(b, Residual || !Raw), b.N, b.rws.ctl,
+        b.rws.tile_excl, b.rws.ex, r.tile, sm);
 }
 
 template <typename Real, bool Residual, bool Raw = false>
@@ -270,7 +274,8 @@ kb_exact_spine(const BatchSlot *slots, const int32_t *work)
     __shared__ SmemExactSpine sm;
     const BatchSlot &b = slots[work[blockIdx.x]];
     k_exact_spine_body<WeightsFromLog<Real>, Residual, Raw>(
-        batch_weights<Real>(b), b.N, b.rws.ctl, b.ntiles, b.rws.ex, sm);
+        batch_weights<Real>(b, Residual || !Raw), b.N, b.rws.ctl, b.ntiles,
+        b.rws.ex, sm);
 }
 
 static __global__ void __launch_bounds__(kSpineThreads)
@@ -336,7 +341,8 @@ union SmemBlockPhase {
     SmemInvert<Residual> inv;
     SmemZeroSpine zsp;
     SmemFill fill;
-    SmemExactTiles ext;
+    SmemExactTiles<Residual> ext;
+    SmemExactTiles<false> ext0;
     SmemExactSpine exs;
 };
 
@@ -423,6 +429,19 @@ kb_block_run(BatchSlot *slots, const BlockItem *items, int n, int *queue,
                 k_cv_finalize_body(a, sm.agg, kBlockMaxTiles, sm.ph.fin);
             }
             __syncthreads();
+            if (WeightsFromLog<Real>::kExactNorm) {
+                // the weights' sequential sum and coefficient
+                const WeightsFromLog<Real> w0 = batch_weights<Real>(b, false);
+                for (int tile = 0; tile < nt; ++tile) {
+                    k_exact_tiles_body<WeightsFromLog<Real>, false, true>(
+                        w0, b.N, b.rws.ctl, b.rws.tile_excl, b.rws.ex, tile,
+                        sm.ph.ext0);
+                    __syncthreads();
+                }
+                k_exact_spine_body<WeightsFromLog<Real>, false, true>(
+                    w0, b.N, b.rws.ctl, nt, b.rws.ex, sm.ph.exs);
+                __syncthreads();
+            }
             const WeightsFromLog<Real> w = batch_weights<Real>(b);
             if (Residual) {
                 for (int tile = 0; tile < nt; ++tile) {
@@ -460,7 +479,7 @@ kb_block_run(BatchSlot *slots, const BlockItem *items, int n, int *queue,
                     __syncthreads();
                 }
             }
-            if (Residual) { // the residuals' exact sum and coefficient
+            if constexpr (Residual) { // the residuals' exact sum
                 for (int tile = 0; tile < nt; ++tile) {
                     k_exact_tiles_body<WeightsFromLog<Real>, true, true>(
                         w, b.N, b.rws.ctl, b.rws.tile_excl, b.rws.ex, tile,
@@ -955,6 +974,13 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
     kb_finalize<<<n, b->max_ntiles <= 256 ? b->tune_final : kFinalThreads, 0,
                   s>>>(sl, work, b->bc);
     int launches = 2;
+    if (WeightsFromLog<Real>::kExactNorm) {
+        // the weights' sequential sum, whose reciprocal normalises them
+        kb_exact_tiles<Real, false, true><<<nt, kThreads, 0, s>>>(sl, map);
+        kb_exact_spine<Real, false, true><<<n, kSpineThreads, 0, s>>>(sl,
+                                                                     work);
+        launches += 2;
+    }
     if (residual) {
         kb_tile_sums<Real, true><<<nt, kThreads, 0, s>>>(sl, map);
         if (sys)

@@ -222,7 +222,8 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
             launch_resample_core(c.scheme, w, N, f->eng, f->rws, nullptr, 0,
                                  /*spine_done=*/true, nullptr,
                                  f->rec_cf + (size_t)f->iter * c.N, s);
-            f->launches += resample_launches(c.scheme, false);
+            f->launches += resample_launches(c.scheme, false,
+                                           WeightsFromLog<Real>::kExactNorm);
         }
         // replay: the recorded ancestry of this step (used only if the
         // recorded decision was to resample)
@@ -244,7 +245,8 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
                         c.N * 4, cudaMemcpyDeviceToDevice, s);
     if (ev)
         cudaEventRecord(ev[2], s);
-    f->launches += 2 + resample_launches(c.scheme, false);
+    f->launches += 2 + resample_launches(c.scheme, false,
+                                           WeightsFromLog<Real>::kExactNorm);
     ++f->iter;
 }
 

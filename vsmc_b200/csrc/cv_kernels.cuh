@@ -634,9 +634,10 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
         sh_coeff = __ddiv_rn(1.0, S1);
     }
     __syncthreads();
-    if (!sh_res || a.residual)
+    if (!sh_res)
         return;
-    // ordered exclusive spine of the normalised shares
+    // ordered exclusive spine of the normalised shares (the residual
+    // schemes' normalisation pass classifies on it too)
     const double coeff = sh_coeff;
     const int per = (nt + blockDim.x - 1) / blockDim.x;
     const int b = threadIdx.x * per, e = min(b + per, nt);
@@ -659,7 +660,7 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
         for (int t = threadIdx.x; t < nt; t += bd)
             a.tile_excl[t] = share[t];
     }
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && !a.residual) {
         ResampleCtl *rc = a.rctl;
         rc->NN = a.N;
         rc->coeff_r = 1.0;

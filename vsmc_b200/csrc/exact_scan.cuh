@@ -14,11 +14,12 @@
 //   rounded to the nearest integer (a tie would depend on the last bit of
 //   S_{i-1}).  Over a run of such "clean" elements the sum is an exact
 //   integer sum.
-// * An approximate prefix G_i with a proven error bound d_i decides which
-//   elements are clean: the binade of G_{i-1} +- d and G_i +- d must be the
-//   same.  |S_i - G_i| <= (i + 1) ulp(S_i) / 2 (each rounding of the
+// * An approximate prefix G_i with a proven error bound d decides which
+//   elements are clean: the windows G_{i-1} +- d and G_i +- d must lie in
+//   one binade.  |S_i - G_i| <= (i + 1) ulp(S_i) / 2 (each rounding of the
 //   sequential sum) + the error of G (a relative margin of the weight
-//   source); d_i = (8 i + 256) ulp(2 max(G, w)) + margin * max(G, w).
+//   source); each thread uses one bound for its kItems elements,
+//   d = (8 i_last + 256) ulp(2 m) + margin * m, m >= every G and w there.
 // * A zero weight while the prefix is still 0 leaves S at 0: clean, k = 0.
 // * The other ("special") elements -- the first, binade crossings,
 //   uncertain binades, ties -- are few (about 40 at N = 2^24): the spine
@@ -26,12 +27,14 @@
 //   over clean runs by their exact integer sums.
 //
 // Phase A (k_exact_tiles_body, per tile): classify, per-tile integer sums,
-// the list of the tile's specials.  Phase B (k_exact_spine_body, one CTA):
+// the list of the tile's specials and, per element, a record: the exact
+// offset of S_i from the S of the tile's last special before it (or of the
+// tile's start), or -1 at a special.  Phase B (k_exact_spine_body, one CTA):
 // the exact S at every tile start and at every special.  Phase C (in
-// k_invert_body): every element's S from its tile's start or its last
-// special plus an integer prefix.  A tile with more than kExactCap specials
+// k_invert_body): S_i = base + record, one exact addition, with no weight,
+// exp or classification.  A tile with more than kExactCap specials
 // (possible only for weights built to create ties) is summed element by
-// element in phase B.
+// element in phase B, which writes S_i itself into its records.
 #pragma once
 
 #include "smc_common.cuh"
@@ -61,75 +64,73 @@ struct ExactScan {
     ExactSpecial *spec;     // ntiles x kExactCap
     double *s_spec;         // ntiles x kExactCap: exact S at each special
     double *start;          // ntiles + 1: exact S before each tile (0 first)
-    double *full;           // N: exact S of the elements of overflow tiles
-    double *s_out;          // ntiles: exact S after each tile with specials
-    unsigned long long *pk; // ntiles + 1: prefix of clean tiles' k_total
-    int32_t *dirty;         // ntiles: the tiles with specials, in order
+    double *rec;            // N: per-element record (see above)
+    int32_t *kint;          // N: floor(N w) (residual schemes)
+    // per tile with specials, by rank (those past the spine's shared stage)
+    double *s_out;          // exact S after the tile
+    unsigned long long *pk; // clean k before the tile
+    int32_t *dirty;         // the tile
+    int32_t *eaft;          // binade of the clean tiles after it
 };
 
 // Binade of a positive normal double: 2^E <= x < 2^(E+1).
 __device__ __forceinline__ int exact_binade(double x)
 {
-    return (int)((__double_as_longlong(x) >> 52) & 0x7ff) - 1023;
+    return ((__double2hiint(x) >> 20) & 0x7ff) - 1023;
 }
 
 // 2^e for -1022 <= e <= 1023.
 __device__ __forceinline__ double exact_pow2(int e)
 {
-    return __longlong_as_double((long long)(e + 1023) << 52);
+    return __hiloint2double((e + 1023) << 20, 0);
 }
 
-struct ExactElem {
-    unsigned long long k;
-    int e;
-    bool special;
-};
-
-// Classification of element i with weight w, approximate prefixes gp
-// (through i - 1) and g (through i), relative margin `rel` of the prefix.
-__device__ __forceinline__ ExactElem exact_classify(long long i, double w,
-                                                    double gp, double g,
-                                                    double rel)
+// Binade shared by every value of [g - d, g + d], or kNoBinade.
+__device__ __forceinline__ int exact_window(double g, double d)
 {
-    ExactElem r;
-    r.k = 0;
-    r.e = kNoBinade;
-    r.special = true;
-    if (i == 0)
-        return r; // S_{-1} = 0: the first addition is the hardware's
-    if (gp == 0.0 && w == 0.0) {
-        // a leading zero: every weight before it is 0 (sums of non-negative
-        // weights vanish only so), S stays 0 and no k accumulates in its run
-        r.special = false;
-        return r;
-    }
-    const double m = fmax(fmax(g, gp), w);
-    if (!(m > 0x1p-960 && m < 0x1p960) || !(w >= 0.0))
-        return r;
-    const double ulp2 = exact_pow2(exact_binade(m) + 1 - 52);
-    const double d = __dadd_rn(__dmul_rn(__dadd_rn(8.0 * (double)i, 256.0),
-                                         ulp2),
-                               __dmul_rn(rel, m));
-    const double plo = __dadd_rn(gp, -d);
-    if (!(plo > 0x1p-960))
-        return r;
-    const double lo = __dadd_rn(g, -d), hi = __dadd_rn(g, d),
-                 phi = __dadd_rn(gp, d);
+    const double lo = __dadd_rn(g, -d), hi = __dadd_rn(g, d);
+    if (!(lo > 0x1p-960))
+        return kNoBinade;
     const int e = exact_binade(hi);
-    if (exact_binade(lo) != e || exact_binade(plo) != e ||
-        exact_binade(phi) != e)
-        return r;
-    // k = w / 2^(e-52), an exact scaling in two power-of-two steps
-    const double kf = __dmul_rn(__dmul_rn(w, 0x1p52), exact_pow2(-e));
-    if (!(kf < 0x1p52))
-        return r;
-    const double fl = floor(kf);
-    if (__dadd_rn(kf, -fl) == 0.5)
-        return r; // a tie: the rounding depends on the sum's last bit
-    r.k = (unsigned long long)rint(kf);
-    r.e = e;
-    r.special = false;
-    return r;
+    return exact_binade(lo) == e ? e : kNoBinade;
+}
+
+// Block-wide exclusive max-scan of one value per thread (0 before the
+// first); `sh` needs blockDim.x/32 entries.
+__device__ __forceinline__ unsigned long long
+block_excl_max(unsigned long long v, unsigned long long *sh)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    unsigned long long inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long n = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o)
+            inc = max(inc, n);
+    }
+    if (lane == 31)
+        sh[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned long long s = lane < nw ? sh[lane] : 0ull;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long n = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o)
+                s = max(s, n);
+        }
+        if (lane < nw)
+            sh[lane] = s;
+    }
+    __syncthreads();
+    unsigned long long ex = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane == 0)
+        ex = 0;
+    if (wid > 0)
+        ex = max(ex, sh[wid - 1]);
+    __syncthreads();
+    return ex;
 }
 
 // The classification of a thread's kItems consecutive elements of a tile
@@ -143,11 +144,14 @@ struct ExactThread {
     int rank0;                        // specials of the tile before j = 0
     int nspec;                        // specials of the tile
     unsigned long long ktile;         // clean k of the tile
+    unsigned long long kb_in;         // kincl at the tile's last special
+                                      // before j = 0 (0: none)
     int e_before;                     // binade of the element before j = 0
 };
 
 struct SmemExactThread {
     unsigned long long shk[kThreads / 32];
+    unsigned long long shm[kThreads / 32];
     int shi[kThreads / 32];
     int elast[kThreads];
 };
@@ -156,8 +160,27 @@ __device__ __forceinline__ void
 exact_thread(long long i0, long long N, const double (&w)[kItems], double a,
              double pre, double rel, ExactThread &x, SmemExactThread &sm)
 {
+    // one error bound for the thread's elements
+    double p = pre, wmax = 0.0;
+    bool bad = false;
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        p += w[j];
+        wmax = fmax(wmax, w[j]);
+        bad |= !(w[j] >= 0.0);
+    }
+    const double m = fmax(__dadd_rn(a, p), wmax);
+    const bool ok = !bad && m > 0x1p-960 && m < 0x1p960;
+    double d = 0.0;
+    if (ok) {
+        const double ulp2 = exact_pow2(exact_binade(m) + 1 - 52);
+        const double il = (double)(i0 + kItems - 1);
+        d = __dadd_rn(__dmul_rn(__dadd_rn(8.0 * il, 256.0), ulp2),
+                      __dmul_rn(rel, m));
+    }
     double gp = __dadd_rn(a, pre);
-    double p = pre;
+    int ep = ok ? exact_window(gp, d) : kNoBinade;
+    p = pre;
     unsigned long long kr = 0;
     int nsp = 0;
     int eprev = kNoBinade;
@@ -168,20 +191,45 @@ exact_thread(long long i0, long long N, const double (&w)[kItems], double a,
         const long long i = i0 + j;
         p += w[j];
         const double g = __dadd_rn(a, p);
+        const int ec = ok ? exact_window(g, d) : kNoBinade;
         if (i < N) {
-            const ExactElem c = exact_classify(i, w[j], gp, g, rel);
-            x.e[j] = c.e;
-            if (c.special) {
+            bool sp = true;
+            unsigned long long k = 0;
+            int e = kNoBinade;
+            if (i == 0) {
+                // S_{-1} = 0: the first addition is the hardware's
+            } else if (gp == 0.0 && w[j] == 0.0) {
+                // a leading zero: every weight before it is 0 (sums of
+                // non-negative weights vanish only so)
+                sp = false;
+            } else if (ec != kNoBinade && ec == ep) {
+                // k = w / 2^(e-52) rounded to nearest: adding 2^52 rounds
+                // it to an integer; a tie depends on the sum's last bit
+                const double kf = __dmul_rn(w[j], exact_pow2(52 - ec));
+                if (kf < 0x1p52) {
+                    const double t = __dadd_rn(kf, 0x1p52);
+                    const double kd = __dadd_rn(t, -0x1p52);
+                    if (fabs(__dadd_rn(kd, -kf)) != 0.5) {
+                        k = (unsigned long long)(__double_as_longlong(t) -
+                                                 __double_as_longlong(0x1p52));
+                        e = ec;
+                        sp = false;
+                    }
+                }
+            }
+            x.e[j] = e;
+            if (sp) {
                 x.special |= 1u << j;
                 ++nsp;
             }
-            kr += c.k;
-            eprev = c.e;
+            kr += k;
+            eprev = e;
         } else {
             x.e[j] = eprev;
         }
         kloc[j] = kr;
         gp = g;
+        ep = ec;
     }
     int nspec;
     x.rank0 = block_excl_scan(nsp, sm.shi, nspec);
@@ -189,9 +237,16 @@ exact_thread(long long i0, long long N, const double (&w)[kItems], double a,
     unsigned long long ktile;
     const unsigned long long kex = block_excl_scan(kr, sm.shk, ktile);
     x.ktile = ktile;
+    unsigned long long vlast = 0;
 #pragma unroll
-    for (int j = 0; j < kItems; ++j)
+    for (int j = 0; j < kItems; ++j) {
         x.kincl[j] = kex + kloc[j];
+        if ((x.special >> j) & 1u)
+            vlast = x.kincl[j];
+    }
+    // kincl is non-decreasing, so the last special before the chunk holds
+    // the largest kincl of the earlier threads' last specials
+    x.kb_in = block_excl_max(vlast, sm.shm);
     sm.elast[threadIdx.x] =
         (x.special >> (kItems - 1)) & 1u ? kNoBinade : x.e[kItems - 1];
     __syncthreads();
@@ -199,13 +254,15 @@ exact_thread(long long i0, long long N, const double (&w)[kItems], double a,
     __syncthreads();
 }
 
-// Phase A: one tile's classification, sums and specials.
+// Phase A: one tile's specials and sums, and the thread's element records
+// (the exact offset from the base, -1 at a special) into `rec`.
 __device__ __forceinline__ void
 exact_tile_record(const ExactThread &x, const double (&w)[kItems],
                   long long base, long long i0, long long N, int tile,
-                  const ExactScan &ex)
+                  const ExactScan &ex, double (&rec)[kItems])
 {
     int r = x.rank0;
+    unsigned long long kb = x.kb_in;
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
         if ((x.special >> j) & 1u) {
@@ -221,49 +278,48 @@ exact_tile_record(const ExactThread &x, const double (&w)[kItems],
                 ex.spec[(size_t)tile * kExactCap + r] = s;
             }
             ++r;
+            kb = x.kincl[j];
+            rec[j] = -1.0;
+        } else {
+            const unsigned long long K = x.kincl[j] - kb;
+            rec[j] = K == 0 ? 0.0
+                            : __dmul_rn((double)K, exact_pow2(x.e[j] - 52));
         }
     }
     const long long last = min(base + (long long)kTile, N) - 1;
-    if (last >= i0 && last < i0 + kItems) {
-        const int j = (int)(last - i0);
-        ex.tiles[tile].e_last =
-            (x.special >> j) & 1u ? kNoBinade : x.e[j];
-    }
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) // (constant indices keep x in registers)
+        if (i0 + j == last)
+            ex.tiles[tile].e_last =
+                (x.special >> j) & 1u ? kNoBinade : x.e[j];
     if (threadIdx.x == 0) {
         ex.tiles[tile].k_total = x.ktile;
         ex.tiles[tile].nspec = x.nspec;
     }
 }
 
-// Phase C: the exact S of a thread's elements from the tile's exact start,
-// its specials' exact values (staged: sv, kb for ranks < kExactCap) and,
-// for an overflow tile, the element values phase B wrote.
+// Phase C: the exact S of a thread's elements from their records, the
+// tile's exact start and its specials' exact values sv (ranks below
+// kExactCap); an overflow tile's records hold S itself.
 __device__ __forceinline__ void
-exact_values(const ExactThread &x, long long i0, double start,
-             const double *sv, const unsigned long long *kb, bool overflow,
-             const double *full, long long N, double (&S)[kItems])
+exact_values(const double (&rec)[kItems], int rank0, double start,
+             const double *sv, bool overflow, double (&S)[kItems])
 {
-    int r = x.rank0 - 1; // rank of the last special before element j
+    int r = rank0 - 1; // rank of the last special before element j
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-        const long long i = i0 + j;
         if (overflow) {
-            S[j] = i < N ? full[i] : 0.0;
+            S[j] = rec[j];
             continue;
         }
-        // r < kExactCap holds when phases A and C classify alike (the same
-        // arithmetic on the same inputs); the clamp keeps the read in bounds
-        if ((x.special >> j) & 1u) {
+        // r < kExactCap holds when the records and the specials come from
+        // one classification; the clamp keeps the read in bounds
+        if (rec[j] < 0.0) {
             ++r;
             S[j] = sv[min(r, kExactCap - 1)];
         } else {
-            const int rc = min(r, kExactCap - 1);
-            const double b = r < 0 ? start : sv[rc];
-            const unsigned long long k0 = r < 0 ? 0ull : kb[rc];
-            const unsigned long long dk = x.kincl[j] - k0;
-            S[j] = dk == 0 ? b
-                           : __dadd_rn(b, __dmul_rn((double)dk,
-                                                    exact_pow2(x.e[j] - 52)));
+            const double b = r < 0 ? start : sv[min(r, kExactCap - 1)];
+            S[j] = __dadd_rn(b, rec[j]);
         }
     }
 }

@@ -1261,7 +1261,7 @@ int vsmc_cuda_gmm_iterate(vsmc_cuda_gmm *g, uint64_t num)
             g->buf[1 - g->cur].base + 13 * N, g->lw, g->ctl, N, (long long)t,
             a, g->gctl, g->hist_accept, g->hist_integrand, g->hist_grid);
         g->cur = 1 - g->cur;
-        g->launches += 4 + resample_launches(scheme, false);
+        g->launches += 4 + resample_launches(scheme, false, true);
         ++g->iter;
     }
     cudaError_t e = cudaGetLastError();

@@ -29,7 +29,10 @@ struct ResampleCtl {
     int active;           // 0: every resample kernel returns at once
     int error;            // sticky vsmc_cuda_status
     long long NN;         // length of the U01 sequence fed to inversion
-    double coeff_r;       // 1 / sum of residuals
+    double coeff_r;       // 1 / sum of residuals (exact once the residuals'
+                          // sequential sum is known)
+    double coeff_r_apx;   // 1 / the spine's sum of residuals
+    double coeff_w;       // 1 / the weights' sequential sum (filters)
     double delta;         // 1 / NN
     double u0;            // systematic start
     long long n_final;    // uniforms consumed by particles 0..N-2
@@ -118,28 +121,54 @@ __device__ __forceinline__ void bin_window(const int32_t *L, int kb,
 // Weight sources --------------------------------------------------------
 // Normalised weights given in memory (generic C ABI).
 struct WeightsGiven {
+    static constexpr bool kExactNorm = false;
     const double *w;
     __device__ __forceinline__ void prepare() {}
     __device__ __forceinline__ double operator()(long long i) const
     {
         return w[i];
     }
+    __device__ __forceinline__ double unnorm(long long i) const
+    {
+        return w[i];
+    }
+    // the approximate spine's scale relative to these weights'
+    __device__ __forceinline__ double spine_ratio() const { return 1.0; }
+    __device__ __forceinline__ double spine_unnorm() const { return 1.0; }
 };
 
-// Weights of a filter: w_i = exp(lw_i - M) * (1 / S1), i.e. the reference's
+// Weights of a filter: w_i = exp(lw_i - M) * coeff, i.e. the reference's
 // normalize_log_weight, vExp and normalize_weight (core/weight_set.hpp:
-// 108-125) evaluated on the fly from raw log-weights.
+// 108-125) evaluated on the fly from raw log-weights.  coeff is 1 / S1 from
+// the tile statistics, or (FP64, `coeff_exact` set) 1 / the sequential sum
+// of exp(lw_i - M) in index order, the reference's `1 / math::asum`
+// (weight_set.hpp:121, math/cblas.hpp:54-63), so that the weights are the
+// reference's bit for bit where exp agrees.
 template <typename Real>
 struct WeightsFromLog {
+    static constexpr bool kExactNorm = sizeof(Real) == sizeof(double);
     const Real *lw;
-    const double *stats; // [0] = M (max log-weight), [1] = S1
-    double M, coeff;
+    const double *stats;       // [0] = M (max log-weight), [1] = S1
+    const double *coeff_exact = nullptr; // the sequential sum's reciprocal
+    double M, coeff, coeff_apx;
     __device__ __forceinline__ void prepare()
     {
         M = stats[0];
-        coeff = __ddiv_rn(1.0, stats[1]);
+        coeff_apx = __ddiv_rn(1.0, stats[1]);
+        coeff = coeff_exact != nullptr ? *coeff_exact : coeff_apx;
     }
     __device__ __forceinline__ double operator()(long long i) const;
+    __device__ __forceinline__ double unnorm(long long i) const;
+    // the approximate spine (tile statistics scaled by coeff_apx) relative
+    // to these weights' scale, and to the unnormalised weights'
+    __device__ __forceinline__ double spine_ratio() const
+    {
+        return coeff_exact != nullptr ? __ddiv_rn(coeff, coeff_apx) : 1.0;
+    }
+    __device__ __forceinline__ double spine_unnorm() const
+    {
+        return stats[1];
+    }
 };
 
 template <>
@@ -147,6 +176,35 @@ __device__ __forceinline__ double
 WeightsFromLog<double>::operator()(long long i) const
 {
     return __dmul_rn(exp(__dadd_rn(lw[i], -M)), coeff);
+}
+
+template <>
+__device__ __forceinline__ double
+WeightsFromLog<double>::unnorm(long long i) const
+{
+    return exp(__dadd_rn(lw[i], -M));
+}
+
+template <>
+__device__ __forceinline__ double
+WeightsFromLog<float>::unnorm(long long i) const
+{
+    return static_cast<double>(expf(lw[i] - static_cast<float>(M)));
+}
+
+// The weight source with the exact normalisation coefficient (held in the
+// control block once the normalisation pass has run), where it has one.
+template <typename W>
+__host__ __device__ inline W with_exact_coeff(W w, const double *)
+{
+    return w;
+}
+template <>
+__host__ __device__ inline WeightsFromLog<double>
+with_exact_coeff(WeightsFromLog<double> w, const double *c)
+{
+    w.coeff_exact = c;
+    return w;
 }
 
 template <>
@@ -208,16 +266,13 @@ struct SmemSortedUniforms {
 };
 template <bool Residual>
 struct SmemInvert {
-    double sw[kTile];                // weights, then uniforms
-    double sk[Residual ? kTile : 1]; // floor(N w) (residual)
+    double sw[kTile];                 // records, then uniforms
+    int32_t sk[Residual ? kTile : 1]; // floor(N w) (residual)
     long long shl[kThreads / 32];
-    double shd[kThreads / 32];
     long long bound[2];
     long long last[kThreads / 32];
-    // the tile's specials of the exact cumulative weight (exact_scan.cuh)
+    // the exact S at the tile's specials (exact_scan.cuh)
     double sv[kExactCap];
-    unsigned long long kb[kExactCap];
-    SmemExactThread et;
 };
 
 // ---------------------------------------------------------------------------
@@ -383,6 +438,7 @@ k_spine_weights_body(const double *tile_sum, const long long *tile_k,
     if (threadIdx.x == 0) {
         ctl->NN = NN;
         ctl->coeff_r = coeff;
+        ctl->coeff_r_apx = coeff;
         ctl->delta = __ddiv_rn(1.0, (double)NN);
         ctl->kbits = bin_kbits(NN);
         ctl->n_final = 0;
@@ -853,37 +909,53 @@ __device__ __forceinline__ long long sys_count(double C, double u0,
 constexpr int kUStage = kTile; // uniforms staged in shared memory per tile
 
 // The weight the inversion scans for element i: w_i, or for the residual
-// schemes its residual r_i * coeff_r (residual.hpp:59-66).
-template <typename W, bool Residual>
+// schemes its residual r_i * coeff_r (residual.hpp:59-66).  Raw: the
+// unnormalised weight exp(lw_i - M) (the normalisation pass), or the
+// residual r_i unscaled (the residuals' sum).
+template <typename W, bool Residual, bool Raw = false>
 __device__ __forceinline__ double scan_weight(const W &wsrc, long long i,
                                               double Nd, double coeff_r,
                                               double *kint)
 {
-    double w = wsrc(i), k = 0.0;
-    if (Residual)
-        w = __dmul_rn(residual_split(w, Nd, k), coeff_r);
+    double w, k = 0.0;
+    if (Raw && !Residual) {
+        w = wsrc.unnorm(i);
+    } else {
+        w = wsrc(i);
+        if (Residual)
+            w = __dmul_rn(residual_split(w, Nd, k), coeff_r);
+    }
     if (kint)
         *kint = k;
     return w;
 }
 
+template <bool Residual>
 struct SmemExactTiles {
-    double sw[kTile];
+    double sw[kTile];                // weights, then the records
+    int32_t sk[Residual ? kTile : 1]; // floor(N w)
     double shd[kThreads / 32];
     SmemExactThread et;
 };
 
 // Phase A of the exact cumulative weight (exact_scan.cuh) for one tile.
-// Raw (residual schemes): the unscaled residuals, whose exact sum is the
-// reference's asum (residual.hpp:63) and so its coefficient.
+// Raw: the weights' or the residuals' sequential sum only (for their
+// coefficient); otherwise also the element records (and, residual, the
+// integer parts floor(N w)) for the inversion.  The approximate spine
+// tile_excl is of the weights (or residuals) scaled by the spine's
+// coefficient: it is rescaled to the weights scanned here.
 template <typename W, bool Residual, bool Raw = false>
 __device__ __forceinline__ void
 k_exact_tiles_body(W wsrc, long long N, const ResampleCtl *ctl,
                    const double *tile_excl, ExactScan ex, int tile,
-                   SmemExactTiles &sm)
+                   SmemExactTiles<Residual> &sm)
 {
-    // residual schemes without residual children scan nothing
-    if (!ctl->active || (Residual && ctl->NN <= 0))
+    if (!ctl->active)
+        return;
+    // residual schemes without residual children scan nothing (the
+    // inversion still takes the integer parts)
+    const bool none = Residual && ctl->NN <= 0;
+    if (none && Raw)
         return;
     wsrc.prepare();
     const long long base = (long long)tile * kTile;
@@ -893,10 +965,22 @@ k_exact_tiles_body(W wsrc, long long N, const ResampleCtl *ctl,
     for (int j = 0; j < kItems; ++j) {
         const int l = j * kThreads + threadIdx.x;
         const long long i = base + l;
-        sm.sw[l] = i < N ? scan_weight<W, Residual>(wsrc, i, Nd, coeff_r,
-                                                    nullptr)
-                         : 0.0;
+        double k = 0.0;
+        const double w = i < N ? scan_weight<W, Residual, Raw>(
+                                     wsrc, i, Nd, coeff_r,
+                                     Residual && !Raw ? &k : nullptr)
+                               : 0.0;
+        if (none) {
+            if (i < N)
+                ex.kint[i] = (int32_t)k;
+            continue;
+        }
+        sm.sw[l] = w;
+        if (Residual && !Raw)
+            sm.sk[l] = (int32_t)k;
     }
+    if (none)
+        return;
     __syncthreads();
     double w[kItems];
     double run = 0.0;
@@ -908,12 +992,35 @@ k_exact_tiles_body(W wsrc, long long N, const ResampleCtl *ctl,
     double total;
     const double pre = block_excl_scan(run, sm.shd, total);
     const long long i0 = base + (long long)threadIdx.x * kItems;
-    // the approximate spine is of the scaled weights; unscaled for Raw
-    const double a_apx = Raw ? __ddiv_rn(tile_excl[tile], ctl->coeff_r)
-                             : tile_excl[tile];
+    double a_apx;
+    if (Residual)
+        a_apx = Raw ? __ddiv_rn(tile_excl[tile], ctl->coeff_r_apx)
+                    : __dmul_rn(tile_excl[tile],
+                                __ddiv_rn(coeff_r, ctl->coeff_r_apx));
+    else
+        a_apx = Raw ? __dmul_rn(tile_excl[tile], wsrc.spine_unnorm())
+                    : __dmul_rn(tile_excl[tile], wsrc.spine_ratio());
     ExactThread x;
     exact_thread(i0, N, w, a_apx, pre, ExactMargin<W>::rel, x, sm.et);
-    exact_tile_record(x, w, base, i0, N, tile, ex);
+    double rec[kItems];
+    exact_tile_record(x, w, base, i0, N, tile, ex, rec);
+    if (!Raw) {
+        // the records (and integer parts) out with coalesced stores
+#pragma unroll
+        for (int j = 0; j < kItems; ++j)
+            sm.sw[threadIdx.x * kItems + j] = rec[j];
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) {
+            const int l = j * kThreads + threadIdx.x;
+            const long long i = base + l;
+            if (i < N) {
+                ex.rec[i] = sm.sw[l];
+                if (Residual)
+                    ex.kint[i] = sm.sk[l];
+            }
+        }
+    }
 }
 
 template <typename W, bool Residual, bool Raw = false>
@@ -921,32 +1028,38 @@ __global__ void __launch_bounds__(kThreads)
 k_exact_tiles(W wsrc, long long N, const ResampleCtl *ctl,
               const double *tile_excl, ExactScan ex)
 {
-    __shared__ SmemExactTiles sm;
+    __shared__ SmemExactTiles<Residual> sm;
     k_exact_tiles_body<W, Residual, Raw>(wsrc, N, ctl, tile_excl, ex,
                                          blockIdx.x, sm);
 }
 
 constexpr int kExactDirtyStage = 256; // tiles with specials the spine stages
 
+// Per tile with specials (its rank q among them, in order): the tile d, its
+// record, the clean k before it (pk: tiles with specials count 0), the
+// binade of the clean tiles after it and the exact S after it.  Ranks below
+// kExactDirtyStage live in shared memory, the others in the ExactScan
+// arrays dirty / pk / eaft / s_out (indexed by q).
 struct SmemExactSpine {
     unsigned long long shk[kSpineThreads / 32];
     int shi[kSpineThreads / 32];
-    int nd;
-    // the walk's inputs, staged (when at most kExactDirtyStage tiles have
-    // specials and their specials fit kExactStage): for the q-th such tile
-    // d, its record, pk[d], pk of the clean run before it and that run's
-    // binade, and its specials at st[st_off[q]...]
-    ExactSpecial st[kExactStage];
-    int st_off[kExactDirtyStage];
     int dq[kExactDirtyStage];
     ExactTile tq[kExactDirtyStage];
-    unsigned long long run_k[kExactDirtyStage];
-    int run_e[kExactDirtyStage];
+    unsigned long long pkq[kExactDirtyStage];
+    int eaft[kExactDirtyStage];
+    double sout[kExactDirtyStage];
+    // the specials of the staged tiles, when they fit: tile q's at
+    // st[st_off[q]...]
+    ExactSpecial st[kExactStage];
+    int st_off[kExactDirtyStage];
 };
 
 // Phase B (one CTA): the exact S before every tile and at every special.
-// Raw: the sum of the unscaled residuals sets coeff_r = 1 / sum, as the
-// reference's `1 / math::asum(M, rptr)` (residual.hpp:63).
+// Each thread owns a contiguous range of tiles; only thread 0's walk over
+// the specials is sequential, and it reads shared memory.  Raw: the
+// sequential sum sets the coefficient -- of the residuals, coeff_r = 1 /
+// sum as the reference's `1 / math::asum(M, rptr)` (residual.hpp:63); of
+// the unnormalised weights, coeff_w (weight_set.hpp:121).
 template <typename W, bool Residual, bool Raw = false>
 __device__ __forceinline__ void
 k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
@@ -956,59 +1069,66 @@ k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
         return;
     wsrc.prepare();
     const int bd = (int)blockDim.x;
-    // prefix of the clean tiles' k (tiles with specials count 0); its
-    // differences are taken in unsigned arithmetic, exact within a run
+    const int per = (nt + bd - 1) / bd;
+    const int tb = min((int)threadIdx.x * per, nt), te = min(tb + per, nt);
+    // 1. prefix of the clean tiles' k and the ranks of the tiles with
+    // specials (tile 0 always has one: its first element)
+    unsigned long long run = 0;
+    int nd = 0;
+    for (int t = tb; t < te; ++t) {
+        const ExactTile et = ex.tiles[t];
+        run += et.nspec == 0 ? et.k_total : 0ull;
+        nd += et.nspec != 0;
+    }
+    unsigned long long ktot;
+    const unsigned long long pk0 = block_excl_scan(run, sm.shk, ktot);
+    int ndt;
+    const int q0 = block_excl_scan(nd, sm.shi, ndt);
     {
-        const int per = (nt + bd - 1) / bd;
-        const int b = threadIdx.x * per, e = min(b + per, nt);
-        unsigned long long run = 0;
-        int nd = 0;
-        for (int t = b; t < e; ++t) {
+        unsigned long long off = pk0;
+        int q = q0;
+        for (int t = tb; t < te; ++t) {
             const ExactTile et = ex.tiles[t];
-            run += et.nspec == 0 ? et.k_total : 0ull;
-            nd += et.nspec != 0;
+            if (et.nspec == 0) {
+                off += et.k_total;
+                continue;
+            }
+            // binade of the clean tiles after t (if the next is clean)
+            int ea = kNoBinade;
+            if (t + 1 < nt) {
+                const ExactTile nx = ex.tiles[t + 1];
+                if (nx.nspec == 0)
+                    ea = nx.e_last;
+            }
+            if (q < kExactDirtyStage) {
+                sm.dq[q] = t;
+                sm.tq[q] = et;
+                sm.pkq[q] = off;
+                sm.eaft[q] = ea;
+            } else {
+                ex.dirty[q] = t;
+                ex.pk[q] = off;
+                ex.eaft[q] = ea;
+            }
+            ++q;
         }
-        unsigned long long tot;
-        unsigned long long off = block_excl_scan(run, sm.shk, tot);
-        int ndt;
-        int doff = block_excl_scan(nd, sm.shi, ndt);
-        for (int t = b; t < e; ++t) {
-            const ExactTile et = ex.tiles[t];
-            ex.pk[t] = off;
-            off += et.nspec == 0 ? et.k_total : 0ull;
-            if (et.nspec != 0)
-                ex.dirty[doff++] = t;
-        }
-        if (threadIdx.x == bd - 1)
-            ex.pk[nt] = off;
-        if (threadIdx.x == 0)
-            sm.nd = ndt;
     }
     __syncthreads();
-    const int nd = sm.nd;
-    // stage the walk's inputs, one tile with specials per thread
-    const bool staged = nd <= kExactDirtyStage;
+    const bool staged_all = ndt <= kExactDirtyStage;
+    // 2. stage the staged tiles' specials when they all fit
     int nsq = 0;
-    if (staged && (int)threadIdx.x < nd) {
-        const int q = threadIdx.x;
-        const int d = ex.dirty[q];
-        const int prev = q > 0 ? ex.dirty[q - 1] : -1;
-        const ExactTile et = ex.tiles[d];
-        sm.dq[q] = d;
-        sm.tq[q] = et;
-        const bool run = d > prev + 1;
-        sm.run_k[q] = run ? ex.pk[d] - ex.pk[prev + 1] : 0ull;
-        sm.run_e[q] = run ? ex.tiles[prev + 1].e_last : kNoBinade;
+    if ((int)threadIdx.x < min(ndt, kExactDirtyStage)) {
+        const ExactTile et = sm.tq[threadIdx.x];
         nsq = et.nspec <= kExactCap ? et.nspec : 0;
     }
     int nst;
-    const int soff = block_excl_scan(nsq, sm.shi, nst);
-    const bool fits = staged && nst <= kExactStage;
-    if (fits && (int)threadIdx.x < nd)
+    const int soff = block_excl_scan(nsq, sm.shi, nst); // ends with a barrier
+    const bool fits = staged_all && nst <= kExactStage;
+    if (fits && (int)threadIdx.x < ndt)
         sm.st_off[threadIdx.x] = soff;
     __syncthreads();
     if (fits) {
-        for (int q = 0; q < nd; ++q) {
+        for (int q = 0; q < ndt; ++q) {
             const int ns = sm.tq[q].nspec;
             if (ns > kExactCap)
                 continue;
@@ -1018,25 +1138,21 @@ k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
         }
     }
     __syncthreads();
+    // 3. the walk over the tiles with specials
     if (threadIdx.x == 0) {
         const double Nd = (double)resample_children(ctl, N);
         const double coeff_r = Residual && !Raw ? ctl->coeff_r : 1.0;
         double S = 0.0;
-        int prev = -1;
-        for (int q = 0; q < nd; ++q) {
-            const int d = staged ? sm.dq[q] : ex.dirty[q];
-            const ExactTile et = staged ? sm.tq[q] : ex.tiles[d];
-            unsigned long long K = 0;
-            int ke = kNoBinade;
-            if (staged) {
-                K = sm.run_k[q];
-                ke = sm.run_e[q];
-            } else if (d > prev + 1) {
-                K = ex.pk[d] - ex.pk[prev + 1];
-                ke = ex.tiles[prev + 1].e_last;
-            }
-            if (K != 0) // the clean tiles prev + 1 .. d - 1
-                S = __dadd_rn(S, __dmul_rn((double)K, exact_pow2(ke - 52)));
+        unsigned long long pk_prev = 0;
+        int ea_prev = kNoBinade;
+        for (int q = 0; q < ndt; ++q) {
+            const bool sq = q < kExactDirtyStage;
+            const int d = sq ? sm.dq[q] : ex.dirty[q];
+            const ExactTile et = sq ? sm.tq[q] : ex.tiles[d];
+            const unsigned long long pkd = sq ? sm.pkq[q] : ex.pk[q];
+            const unsigned long long K = pkd - pk_prev;
+            if (K != 0) // the clean tiles between the previous and d
+                S = __dadd_rn(S, __dmul_rn((double)K, exact_pow2(ea_prev - 52)));
             ex.start[d] = S;
             if (et.nspec <= kExactCap) {
                 unsigned long long kb = 0;
@@ -1061,39 +1177,56 @@ k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
                 const long long b0 = (long long)d * kTile;
                 const long long b1 = min(b0 + (long long)kTile, N);
                 for (long long i = b0; i < b1; ++i) {
-                    S = __dadd_rn(S, scan_weight<W, Residual>(
+                    S = __dadd_rn(S, scan_weight<W, Residual, Raw>(
                                          wsrc, i, Nd, coeff_r, nullptr));
-                    ex.full[i] = S;
+                    if (!Raw)
+                        ex.rec[i] = S;
                 }
             }
-            ex.s_out[d] = S;
-            prev = d;
+            if (sq)
+                sm.sout[q] = S;
+            else
+                ex.s_out[q] = S;
+            pk_prev = pkd;
+            ea_prev = sq ? sm.eaft[q] : ex.eaft[q];
         }
     }
     __syncthreads();
-    // every clean tile and the end: the last tile with specials before it
-    // (tile 0 always has one: its first element) plus the exact run sum
-    for (int t = threadIdx.x; t <= nt; t += bd) {
-        if (t < nt && ex.tiles[t].nspec != 0)
-            continue;
-        int lo = 0, hi = nd - 1; // last q with dirty[q] < t
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (ex.dirty[mid] < t)
-                lo = mid;
-            else
-                hi = mid - 1;
+    // 4. every clean tile (and the end): the exact S after the last tile
+    // with specials before it plus the clean k since, in that binade
+    {
+        unsigned long long off = pk0;
+        int q = q0 - 1; // rank of the last tile with specials before tb
+        const auto after = [&](int qq, unsigned long long k) {
+            if (qq < 0) // (tile 0 always has a special)
+                return 0.0;
+            const bool sq = qq < kExactDirtyStage;
+            double S = sq ? sm.sout[qq] : ex.s_out[qq];
+            const unsigned long long K =
+                k - (sq ? sm.pkq[qq] : ex.pk[qq]);
+            if (K != 0) {
+                const int ea = sq ? sm.eaft[qq] : ex.eaft[qq];
+                S = __dadd_rn(S, __dmul_rn((double)K, exact_pow2(ea - 52)));
+            }
+            return S;
+        };
+        for (int t = tb; t < te; ++t) {
+            const ExactTile et = ex.tiles[t];
+            if (et.nspec != 0) {
+                ++q;
+                continue;
+            }
+            ex.start[t] = after(q, off);
+            off += et.k_total;
         }
-        const int d = ex.dirty[lo];
-        const unsigned long long K = ex.pk[t] - ex.pk[d + 1];
-        double S = ex.s_out[d];
-        if (K != 0)
-            S = __dadd_rn(S, __dmul_rn((double)K,
-                                       exact_pow2(ex.tiles[d + 1].e_last -
-                                                  52)));
-        ex.start[t] = S;
-        if (Raw && t == nt)
-            ctl->coeff_r = __ddiv_rn(1.0, S);
+        if (tb < te && te == nt) {
+            const double S = after(q, off);
+            ex.start[nt] = S;
+            if (Raw && Residual)
+                ctl->coeff_r = __ddiv_rn(1.0, S);
+            else if (Raw)
+                ctl->coeff_w = __ddiv_rn(1.0, S);
+        }
     }
 }
 
@@ -1122,30 +1255,26 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
 {
     if (!ctl->active)
         return;
-    double *sw = sm.sw; // weights, then uniforms
-    double *sk = sm.sk; // floor(N w) (residual)
+    double *sw = sm.sw;  // records, then uniforms
+    int32_t *sk = sm.sk; // floor(N w) (residual)
     long long *shl = sm.shl;
-    double *shd = sm.shd;
     long long *sh_bound = sm.bound;
     long long *sh_last = sm.last;
-    wsrc.prepare();
+    (void)wsrc; // the weights enter through the exact scan's records
 
     const int tile = tile_bid;
     const long long base = (long long)tile * kTile;
     const long long NN = ctl->NN;
     const long long Nout = resample_children(ctl, N);
-    const double Nd = (double)Nout;
-    const double coeff_r = Residual ? ctl->coeff_r : 1.0;
     const double u0 = Sys ? ctl->u0 : 0.0;
     const double delta = ctl->delta;
     const long long nu = Sys ? NN : min(NN, n_u);
     // the reference's cumulative weight before and at the end of the tile,
-    // exactly (exact_scan.cuh); the approximate spine classifies.  Residual
-    // schemes without residual children draw no uniform and scan nothing.
+    // exactly (exact_scan.cuh).  Residual schemes without residual children
+    // draw no uniform and scan nothing.
     const bool exact = !(Residual && NN <= 0);
     const double a = exact ? ex.start[tile] : 0.0;
     const double b = exact ? ex.start[tile + 1] : 0.0;
-    const double a_apx = tile_excl[tile];
     const int nsp_tile = exact ? ex.tiles[tile].nspec : 0;
 
     // uniforms that can fall in this tile: (ub(a), ub(b)], each found in a
@@ -1154,43 +1283,36 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     if (wid < 2) {
         const double C = wid == 0 ? a : b;
         long long r;
-        if (wid == 0 && tile == 0) {
-            r = 0;
+        if ((wid == 0 && tile == 0) || nu <= 0) {
+            r = 0; // (no uniform: the bin index L is not written)
         } else if (Sys) {
             r = sys_count(C, u0, delta, NN);
         } else {
             long long wl, wh;
             bin_window(L, ctl->kbits, nu, C, wl, wh);
-            wl = min(wl, nu);
+            wl = max(min(wl, nu), 0ll);
             wh = min(max(wh, wl), nu);
             r = warp_upper_bound([u](long long i) { return u[i]; }, wl, wh, C);
         }
         if ((threadIdx.x & 31) == 0)
             sh_bound[wid] = r;
     }
-    // striped (coalesced) load of the tile's weights into shared memory
+    // striped (coalesced) load of the tile's records (and integer parts)
+    // into shared memory
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
         const int l = j * kThreads + threadIdx.x;
         const long long i = base + l;
-        double w = 0.0, k = 0.0;
-        if (i < N) {
-            w = wsrc(i);
-            if (Residual)
-                w = __dmul_rn(residual_split(w, Nd, k), coeff_r);
-        }
-        sw[l] = w;
+        if (exact)
+            sw[l] = i < N ? ex.rec[i] : 0.0;
         if (Residual)
-            sk[l] = k;
+            sk[l] = i < N ? ex.kint[i] : 0;
     }
-    if (nsp_tile <= kExactCap && (int)threadIdx.x < nsp_tile) {
-        const size_t q = (size_t)tile * kExactCap + threadIdx.x;
-        sm.sv[threadIdx.x] = ex.s_spec[q];
-        sm.kb[threadIdx.x] = ex.spec[q].k_before;
-    }
+    if (nsp_tile <= kExactCap && (int)threadIdx.x < nsp_tile)
+        sm.sv[threadIdx.x] = ex.s_spec[(size_t)tile * kExactCap + threadIdx.x];
     __syncthreads();
     // the tile's uniforms are loaded into registers now and written to
-    // shared memory after the scan, so their latency overlaps the scan
+    // shared memory after the records are read
     const long long lo = sh_bound[0];
     const long long hi = max(sh_bound[1], lo);
     const bool staged = !Sys && (hi - lo) <= kUStage;
@@ -1202,26 +1324,25 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
             upre[j] = n < hi ? u[n] : 0.0;
         }
     }
-    double wv[kItems];
-    double run = 0.0;
-#pragma unroll
-    for (int j = 0; j < kItems; ++j) {
-        wv[j] = sw[threadIdx.x * kItems + j];
-        run += wv[j];
-    }
-    double total;
-    const double pre = block_excl_scan(run, shd, total); // ends with a barrier
     // each particle's cumulative weight, exactly the reference's
     double Cx[kItems];
 #pragma unroll
     for (int j = 0; j < kItems; ++j)
         Cx[j] = 0.0;
     if (exact) {
-        ExactThread x;
-        exact_thread(base + (long long)threadIdx.x * kItems, N, wv, a_apx, pre,
-                     ExactMargin<W>::rel, x, sm.et);
-        exact_values(x, base + (long long)threadIdx.x * kItems, a, sm.sv,
-                     sm.kb, nsp_tile > kExactCap, ex.full, N, Cx);
+        double rv[kItems];
+        int nsp = 0;
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) {
+            rv[j] = sw[threadIdx.x * kItems + j];
+            nsp += rv[j] < 0.0;
+        }
+        int nspec;
+        const int rank0 = block_excl_scan(nsp, reinterpret_cast<int *>(shl),
+                                          nspec); // ends with a barrier
+        exact_values(rv, rank0, a, sm.sv, nsp_tile > kExactCap, Cx);
+    } else {
+        __syncthreads();
     }
     if (staged) {
 #pragma unroll
@@ -1664,7 +1785,8 @@ constexpr size_t exact_scan_bytes(long long N)
     return align256(nt * sizeof(ExactTile)) +
            align256(nt * kExactCap * sizeof(ExactSpecial)) +
            align256(nt * kExactCap * 8) + 3 * align256(nt * 8) +
-           align256((size_t)N * 8) + align256(nt * 4);
+           align256((size_t)N * 8) + align256((size_t)N * 4) +
+           2 * align256(nt * 4);
 }
 
 constexpr size_t resample_workspace_bytes(long long N)
@@ -1723,14 +1845,19 @@ inline ResampleWorkspace carve_workspace(void *base, long long N)
     p += align256(nt * 8);
     w.ex.pk = reinterpret_cast<unsigned long long *>(p);
     p += align256(nt * 8);
-    w.ex.full = reinterpret_cast<double *>(p);
+    w.ex.rec = reinterpret_cast<double *>(p);
     p += align256((size_t)N * 8);
+    w.ex.kint = reinterpret_cast<int32_t *>(p);
+    p += align256((size_t)N * 4);
     w.ex.dirty = reinterpret_cast<int32_t *>(p);
+    p += align256(nt * 4);
+    w.ex.eaft = reinterpret_cast<int32_t *>(p);
     return w;
 }
 
-// Kernels launch_resample_core issues (for the launch counters).
-inline int resample_launches(int scheme, bool parity)
+// Kernels launch_resample_core issues (for the launch counters); the
+// filters' FP64 weights add the normalisation pass (exact_norm).
+inline int resample_launches(int scheme, bool parity, bool exact_norm = false)
 {
     const bool residual = scheme == VSMC_CUDA_RESIDUAL ||
                           scheme == VSMC_CUDA_RESIDUAL_STRATIFIED ||
@@ -1743,6 +1870,8 @@ inline int resample_launches(int scheme, bool parity)
                // position), cfrp fill
     if (residual)
         n += 4; // tile sums, spine, the residuals' exact sum
+    if (exact_norm)
+        n += 2;
     if (parity)
         n += 2;
     else if (strat)
@@ -1775,8 +1904,31 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
                      scheme == VSMC_CUDA_RESIDUAL_SYSTEMATIC;
     const bool strat = scheme == VSMC_CUDA_STRATIFIED ||
                        scheme == VSMC_CUDA_RESIDUAL_STRATIFIED;
+    // the filters' FP64 weights: first the sequential sum of exp(lw - M),
+    // whose reciprocal normalises them (on the approximate spine of the
+    // weights, drawn here when the caller has none)
+    W wx = wsrc;
+    if (W::kExactNorm) {
+        if (!spine_done) {
+            k_tile_sums<W, false><<<nt, kThreads, 0, s>>>(
+                wsrc, N, ws.ctl, ws.tile_sum, nullptr);
+            if (sys)
+                k_spine_weights<false, true><<<1, kSpineThreads, 0, s>>>(
+                    ws.tile_sum, nullptr, ws.tile_excl, nullptr, nt, N, eng,
+                    ws.ctl);
+            else
+                k_spine_weights<false, false><<<1, kSpineThreads, 0, s>>>(
+                    ws.tile_sum, nullptr, ws.tile_excl, nullptr, nt, N, eng,
+                    ws.ctl);
+        }
+        k_exact_tiles<W, false, true><<<nt, kThreads, 0, s>>>(
+            wsrc, N, ws.ctl, ws.tile_excl, ws.ex);
+        k_exact_spine<W, false, true><<<1, kSpineThreads, 0, s>>>(
+            wsrc, N, ws.ctl, nt, ws.ex);
+        wx = with_exact_coeff(wsrc, &ws.ctl->coeff_w);
+    }
     if (residual) {
-        k_tile_sums<W, true><<<nt, kThreads, 0, s>>>(wsrc, N, ws.ctl,
+        k_tile_sums<W, true><<<nt, kThreads, 0, s>>>(wx, N, ws.ctl,
                                                     ws.tile_sum, ws.tile_k);
         if (sys)
             k_spine_weights<true, true><<<1, kSpineThreads, 0, s>>>(
@@ -1786,8 +1938,8 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
             k_spine_weights<true, false><<<1, kSpineThreads, 0, s>>>(
                 ws.tile_sum, ws.tile_k, ws.tile_excl, ws.tile_kexcl, nt, N,
                 eng, ws.ctl);
-    } else if (!spine_done) {
-        k_tile_sums<W, false><<<nt, kThreads, 0, s>>>(wsrc, N, ws.ctl,
+    } else if (!spine_done && !W::kExactNorm) {
+        k_tile_sums<W, false><<<nt, kThreads, 0, s>>>(wx, N, ws.ctl,
                                                      ws.tile_sum, nullptr);
         if (sys)
             k_spine_weights<false, true><<<1, kSpineThreads, 0, s>>>(
@@ -1830,22 +1982,22 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
     // scales them)
     if (residual) {
         k_exact_tiles<W, true, true><<<nt, kThreads, 0, s>>>(
-            wsrc, N, ws.ctl, ws.tile_excl, ws.ex);
+            wx, N, ws.ctl, ws.tile_excl, ws.ex);
         k_exact_spine<W, true, true><<<1, kSpineThreads, 0, s>>>(
-            wsrc, N, ws.ctl, nt, ws.ex);
-        k_exact_tiles<W, true><<<nt, kThreads, 0, s>>>(wsrc, N, ws.ctl,
+            wx, N, ws.ctl, nt, ws.ex);
+        k_exact_tiles<W, true><<<nt, kThreads, 0, s>>>(wx, N, ws.ctl,
                                                        ws.tile_excl, ws.ex);
-        k_exact_spine<W, true><<<1, kSpineThreads, 0, s>>>(wsrc, N, ws.ctl,
+        k_exact_spine<W, true><<<1, kSpineThreads, 0, s>>>(wx, N, ws.ctl,
                                                            nt, ws.ex);
     } else {
-        k_exact_tiles<W, false><<<nt, kThreads, 0, s>>>(wsrc, N, ws.ctl,
+        k_exact_tiles<W, false><<<nt, kThreads, 0, s>>>(wx, N, ws.ctl,
                                                         ws.tile_excl, ws.ex);
-        k_exact_spine<W, false><<<1, kSpineThreads, 0, s>>>(wsrc, N, ws.ctl,
+        k_exact_spine<W, false><<<1, kSpineThreads, 0, s>>>(wx, N, ws.ctl,
                                                             nt, ws.ex);
     }
 #define VSMC_INVERT(R, S)                                                     \
     k_invert<W, R, S><<<nt, kThreads, 0, s>>>(                                \
-        wsrc, N, ws.ctl, ws.tile_excl, kex, u, n_u, ws.bins, rep_out,        \
+        wx, N, ws.ctl, ws.tile_excl, kex, u, n_u, ws.bins, rep_out,        \
         copy_from, ws.sinc, ws.tile_zeros, ws.tile_sinc_last, ws.ex)
     if (residual && sys)
         VSMC_INVERT(true, true);

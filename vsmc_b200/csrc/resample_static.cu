@@ -11,7 +11,7 @@
 //
 // The scratch is one file-scope __device__ array sized for at most
 // VSMC_CUDA_NOALLOC_MAX_N particles.  Every GPU that loads the library keeps
-// it (about 4.1 MiB) until the process exits.  All calls share it and it
+// it (about 7.4 MiB) until the process exits.  All calls share it and it
 // keeps the previous call's contents: each call rewrites the control block
 // from the host and every other array is fully written before it is read,
 // so nothing stale is used, but two calls that overlap on the GPU (for

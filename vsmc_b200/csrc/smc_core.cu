@@ -276,7 +276,7 @@ int vsmc_cuda_smc_finish_step(vsmc_cuda_smc *s)
     launch_resample_core(sch, w, N, s->eng, s->rws, nullptr, 0,
                          /*spine_done=*/true, nullptr, s->copy_from,
                          s->stream);
-    s->launches += 1 + resample_launches(sch, false);
+    s->launches += 1 + resample_launches(sch, false, true);
     ++s->iter;
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? VSMC_CUDA_OK
