@@ -89,7 +89,8 @@ __device__ __forceinline__ MoveArgs<Real> batch_move_args(const BatchSlot &b,
 }
 
 // A slot's weights; `normed`: with the exact normalisation coefficient of
-// the FP64 form (after its normalisation pass).
+// the FP64 form and the unnormalised weights its normalisation pass kept
+// (after that pass).
 template <typename Real>
 __device__ __forceinline__ WeightsFromLog<Real> batch_weights(
     const BatchSlot &b, bool normed = true)
@@ -98,7 +99,7 @@ __device__ __forceinline__ WeightsFromLog<Real> batch_weights(
     w.lw = static_cast<const Real *>(b.lw);
     w.stats = &b.ctl->lw_max;
     if (normed)
-        w = with_exact_coeff(w, &b.rws.ctl->coeff_w);
+        w = with_exact_coeff(w, &b.rws.ctl->coeff_w, b.rws.ex.rec);
     return w;
 }
 

@@ -179,57 +179,83 @@ exact_thread(long long i0, long long N, const double (&w)[kItems], double a,
                       __dmul_rn(rel, m));
     }
     double gp = __dadd_rn(a, pre);
-    int ep = ok ? exact_window(gp, d) : kNoBinade;
-    p = pre;
     unsigned long long kr = 0;
     int nsp = 0;
-    int eprev = kNoBinade;
     unsigned long long kloc[kItems];
     x.special = 0;
+    // the common case: the windows of the thread's first and last prefix
+    // lie in one binade, so every window between them does and each of
+    // the thread's elements is clean (unless a tie)
+    bool fast = false;
+    if (ok && i0 > 0 && i0 + kItems <= N) {
+        const int e0 = exact_window(gp, d);
+        if (e0 != kNoBinade && e0 == exact_window(__dadd_rn(a, p), d)) {
+            const double sc = exact_pow2(52 - e0);
+            bool slow = false;
 #pragma unroll
-    for (int j = 0; j < kItems; ++j) {
-        const long long i = i0 + j;
-        p += w[j];
-        const double g = __dadd_rn(a, p);
-        const int ec = ok ? exact_window(g, d) : kNoBinade;
-        if (i < N) {
-            bool sp = true;
-            unsigned long long k = 0;
-            int e = kNoBinade;
-            if (i == 0) {
-                // S_{-1} = 0: the first addition is the hardware's
-            } else if (gp == 0.0 && w[j] == 0.0) {
-                // a leading zero: every weight before it is 0 (sums of
-                // non-negative weights vanish only so)
-                sp = false;
-            } else if (ec != kNoBinade && ec == ep) {
-                // k = w / 2^(e-52) rounded to nearest: adding 2^52 rounds
-                // it to an integer; a tie depends on the sum's last bit
-                const double kf = __dmul_rn(w[j], exact_pow2(52 - ec));
-                if (kf < 0x1p52) {
-                    const double t = __dadd_rn(kf, 0x1p52);
-                    const double kd = __dadd_rn(t, -0x1p52);
-                    if (fabs(__dadd_rn(kd, -kf)) != 0.5) {
-                        k = (unsigned long long)(__double_as_longlong(t) -
-                                                 __double_as_longlong(0x1p52));
-                        e = ec;
-                        sp = false;
+            for (int j = 0; j < kItems; ++j) {
+                const double kf = __dmul_rn(w[j], sc);
+                const double t = __dadd_rn(kf, 0x1p52);
+                slow |= !(kf < 0x1p52) ||
+                        fabs(__dadd_rn(__dadd_rn(t, -0x1p52), -kf)) == 0.5;
+                kr += (unsigned long long)(__double_as_longlong(t) -
+                                           __double_as_longlong(0x1p52));
+                kloc[j] = kr;
+                x.e[j] = e0;
+            }
+            fast = !slow;
+        }
+    }
+    int ep = ok && !fast ? exact_window(gp, d) : kNoBinade;
+    p = pre;
+    int eprev = kNoBinade;
+    if (!fast) {
+        kr = 0;
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) {
+            const long long i = i0 + j;
+            p += w[j];
+            const double g = __dadd_rn(a, p);
+            const int ec = ok ? exact_window(g, d) : kNoBinade;
+            if (i < N) {
+                bool sp = true;
+                unsigned long long k = 0;
+                int e = kNoBinade;
+                if (i == 0) {
+                    // S_{-1} = 0: the first addition is the hardware's
+                } else if (gp == 0.0 && w[j] == 0.0) {
+                    // a leading zero: every weight before it is 0 (sums of
+                    // non-negative weights vanish only so)
+                    sp = false;
+                } else if (ec != kNoBinade && ec == ep) {
+                    // k = w / 2^(e-52) rounded to nearest: adding 2^52 rounds
+                    // it to an integer; a tie depends on the sum's last bit
+                    const double kf = __dmul_rn(w[j], exact_pow2(52 - ec));
+                    if (kf < 0x1p52) {
+                        const double t = __dadd_rn(kf, 0x1p52);
+                        const double kd = __dadd_rn(t, -0x1p52);
+                        if (fabs(__dadd_rn(kd, -kf)) != 0.5) {
+                            k = (unsigned long long)(__double_as_longlong(t) -
+                                                     __double_as_longlong(0x1p52));
+                            e = ec;
+                            sp = false;
+                        }
                     }
                 }
+                x.e[j] = e;
+                if (sp) {
+                    x.special |= 1u << j;
+                    ++nsp;
+                }
+                kr += k;
+                eprev = e;
+            } else {
+                x.e[j] = eprev;
             }
-            x.e[j] = e;
-            if (sp) {
-                x.special |= 1u << j;
-                ++nsp;
-            }
-            kr += k;
-            eprev = e;
-        } else {
-            x.e[j] = eprev;
+            kloc[j] = kr;
+            gp = g;
+            ep = ec;
         }
-        kloc[j] = kr;
-        gp = g;
-        ep = ec;
     }
     int nspec;
     x.rank0 = block_excl_scan(nsp, sm.shi, nspec);

@@ -150,6 +150,7 @@ struct WeightsFromLog {
     const Real *lw;
     const double *stats;       // [0] = M (max log-weight), [1] = S1
     const double *coeff_exact = nullptr; // the sequential sum's reciprocal
+    const double *raw = nullptr; // exp(lw_i - M), kept by that pass
     double M, coeff, coeff_apx;
     __device__ __forceinline__ void prepare()
     {
@@ -173,16 +174,16 @@ struct WeightsFromLog {
 
 template <>
 __device__ __forceinline__ double
-WeightsFromLog<double>::operator()(long long i) const
+WeightsFromLog<double>::unnorm(long long i) const
 {
-    return __dmul_rn(exp(__dadd_rn(lw[i], -M)), coeff);
+    return raw != nullptr ? raw[i] : exp(__dadd_rn(lw[i], -M));
 }
 
 template <>
 __device__ __forceinline__ double
-WeightsFromLog<double>::unnorm(long long i) const
+WeightsFromLog<double>::operator()(long long i) const
 {
-    return exp(__dadd_rn(lw[i], -M));
+    return __dmul_rn(unnorm(i), coeff);
 }
 
 template <>
@@ -193,17 +194,20 @@ WeightsFromLog<float>::unnorm(long long i) const
 }
 
 // The weight source with the exact normalisation coefficient (held in the
-// control block once the normalisation pass has run), where it has one.
+// control block once the normalisation pass has run) and the unnormalised
+// weights that pass kept, where it has them.
 template <typename W>
-__host__ __device__ inline W with_exact_coeff(W w, const double *)
+__host__ __device__ inline W with_exact_coeff(W w, const double *,
+                                              const double *)
 {
     return w;
 }
 template <>
 __host__ __device__ inline WeightsFromLog<double>
-with_exact_coeff(WeightsFromLog<double> w, const double *c)
+with_exact_coeff(WeightsFromLog<double> w, const double *c, const double *raw)
 {
     w.coeff_exact = c;
+    w.raw = raw;
     return w;
 }
 
@@ -264,10 +268,31 @@ struct SmemSortedUniforms {
     double sh[kThreads / 32];
     double shm[kThreads];
 };
+// Uniforms staged in shared memory per tile: twice the expected count, so
+// that only a tile holding more than twice its share searches global memory.
+constexpr int kUStage = 2 * kTile;
+
+// Asynchronous 8-byte global-to-shared copies (cp.async): the tile's
+// uniforms travel while the threads work on their records.
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit()
+{
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 template <bool Residual>
 struct SmemInvert {
-    double sw[kTile];                 // records, then uniforms
-    int32_t sk[Residual ? kTile : 1]; // floor(N w) (residual)
+    double sw[kUStage];               // uniforms, then the outputs
     long long shl[kThreads / 32];
     long long bound[2];
     long long last[kThreads / 32];
@@ -853,6 +878,22 @@ __device__ __forceinline__ long long ub_global(const double *u, long long lo,
     return lo;
 }
 
+// ub_gallop over global memory: the count from a known count c <= it.
+__device__ __forceinline__ long long ub_gallop_global(const double *u,
+                                                      long long c,
+                                                      long long n, double C)
+{
+    long long lo = c, step = 1;
+    while (lo < n) {
+        const long long p = min(lo + step - 1, n - 1);
+        if (u[p] > C)
+            return ub_global(u, lo, p, C);
+        lo = p + 1;
+        step <<= 1;
+    }
+    return n;
+}
+
 // Warp-cooperative upper bound over a non-decreasing sequence f(0..n-1):
 // each round the 32 lanes probe 32 evenly spaced points, so a range of n
 // shrinks by 33x per global-memory round trip.  Every lane returns the
@@ -906,7 +947,7 @@ __device__ __forceinline__ long long sys_count(double C, double u0,
     return n;
 }
 
-constexpr int kUStage = kTile; // uniforms staged in shared memory per tile
+
 
 // The weight the inversion scans for element i: w_i, or for the residual
 // schemes its residual r_i * coeff_r (residual.hpp:59-66).  Raw: the
@@ -978,6 +1019,8 @@ k_exact_tiles_body(W wsrc, long long N, const ResampleCtl *ctl,
         sm.sw[l] = w;
         if (Residual && !Raw)
             sm.sk[l] = (int32_t)k;
+        if (Raw && !Residual && W::kExactNorm && i < N)
+            ex.rec[i] = w; // the unnormalised weights, for the later passes
     }
     if (none)
         return;
@@ -1005,7 +1048,10 @@ k_exact_tiles_body(W wsrc, long long N, const ResampleCtl *ctl,
     double rec[kItems];
     exact_tile_record(x, w, base, i0, N, tile, ex, rec);
     if (!Raw) {
-        // the records (and integer parts) out with coalesced stores
+        // the records (and integer parts) out with coalesced stores; a tile
+        // with more specials than kept keeps its unnormalised weights for
+        // the spine, which writes S itself there
+        const bool overflow = x.nspec > kExactCap;
 #pragma unroll
         for (int j = 0; j < kItems; ++j)
             sm.sw[threadIdx.x * kItems + j] = rec[j];
@@ -1015,7 +1061,8 @@ k_exact_tiles_body(W wsrc, long long N, const ResampleCtl *ctl,
             const int l = j * kThreads + threadIdx.x;
             const long long i = base + l;
             if (i < N) {
-                ex.rec[i] = sm.sw[l];
+                if (!overflow)
+                    ex.rec[i] = sm.sw[l];
                 if (Residual)
                     ex.kint[i] = sm.sk[l];
             }
@@ -1073,12 +1120,22 @@ k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
     const int tb = min((int)threadIdx.x * per, nt), te = min(tb + per, nt);
     // 1. prefix of the clean tiles' k and the ranks of the tiles with
     // specials (tile 0 always has one: its first element)
+    // (the tile records are read eight at a time, so that their loads
+    // overlap)
     unsigned long long run = 0;
     int nd = 0;
-    for (int t = tb; t < te; ++t) {
-        const ExactTile et = ex.tiles[t];
-        run += et.nspec == 0 ? et.k_total : 0ull;
-        nd += et.nspec != 0;
+    for (int t0 = tb; t0 < te; t0 += 8) {
+        ExactTile et[8];
+#pragma unroll
+        for (int v = 0; v < 8; ++v)
+            if (t0 + v < te)
+                et[v] = ex.tiles[t0 + v];
+#pragma unroll
+        for (int v = 0; v < 8; ++v)
+            if (t0 + v < te) {
+                run += et[v].nspec == 0 ? et[v].k_total : 0ull;
+                nd += et[v].nspec != 0;
+            }
     }
     unsigned long long ktot;
     const unsigned long long pk0 = block_excl_scan(run, sm.shk, ktot);
@@ -1087,8 +1144,18 @@ k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
     {
         unsigned long long off = pk0;
         int q = q0;
-        for (int t = tb; t < te; ++t) {
-            const ExactTile et = ex.tiles[t];
+        for (int t0 = tb; t0 < te; t0 += 8) {
+          ExactTile ev[8];
+#pragma unroll
+          for (int v = 0; v < 8; ++v)
+              if (t0 + v < te)
+                  ev[v] = ex.tiles[t0 + v];
+#pragma unroll
+          for (int v = 0; v < 8; ++v) {
+            const int t = t0 + v;
+            if (t >= te)
+                break;
+            const ExactTile et = ev[v];
             if (et.nspec == 0) {
                 off += et.k_total;
                 continue;
@@ -1111,6 +1178,7 @@ k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
                 ex.eaft[q] = ea;
             }
             ++q;
+          }
         }
     }
     __syncthreads();
@@ -1127,12 +1195,13 @@ k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
     if (fits && (int)threadIdx.x < ndt)
         sm.st_off[threadIdx.x] = soff;
     __syncthreads();
-    if (fits) {
-        for (int q = 0; q < ndt; ++q) {
+    if (fits) { // a warp per tile with specials
+        const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+        for (int q = wq; q < ndt; q += bd >> 5) {
             const int ns = sm.tq[q].nspec;
             if (ns > kExactCap)
                 continue;
-            for (int r = threadIdx.x; r < ns; r += bd)
+            for (int r = lane; r < ns; r += 32)
                 sm.st[sm.st_off[q] + r] =
                     ex.spec[(size_t)sm.dq[q] * kExactCap + r];
         }
@@ -1210,14 +1279,23 @@ k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
             }
             return S;
         };
-        for (int t = tb; t < te; ++t) {
-            const ExactTile et = ex.tiles[t];
-            if (et.nspec != 0) {
-                ++q;
-                continue;
+        for (int t0 = tb; t0 < te; t0 += 8) {
+            ExactTile et[8];
+#pragma unroll
+            for (int v = 0; v < 8; ++v)
+                if (t0 + v < te)
+                    et[v] = ex.tiles[t0 + v];
+#pragma unroll
+            for (int v = 0; v < 8; ++v) {
+                if (t0 + v >= te)
+                    break;
+                if (et[v].nspec != 0) {
+                    ++q;
+                    continue;
+                }
+                ex.start[t0 + v] = after(q, off);
+                off += et[v].k_total;
             }
-            ex.start[t] = after(q, off);
-            off += et.k_total;
         }
         if (tb < te && te == nt) {
             const double S = after(q, off);
@@ -1255,8 +1333,7 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
 {
     if (!ctl->active)
         return;
-    double *sw = sm.sw;  // records, then uniforms
-    int32_t *sk = sm.sk; // floor(N w) (residual)
+    double *sw = sm.sw; // uniforms, then the outputs
     long long *shl = sm.shl;
     long long *sh_bound = sm.bound;
     long long *sh_last = sm.last;
@@ -1297,32 +1374,48 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
         if ((threadIdx.x & 31) == 0)
             sh_bound[wid] = r;
     }
-    // striped (coalesced) load of the tile's records (and integer parts)
-    // into shared memory
+    // the thread's records and integer parts, straight into registers
+    // (kItems consecutive values: vector loads; the arrays are padded past
+    // N to a multiple of 32 elements)
+    const long long i0l = base + (long long)threadIdx.x * kItems;
+    double rv[kItems];
+    int k_int[kItems];
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-        const int l = j * kThreads + threadIdx.x;
-        const long long i = base + l;
-        if (exact)
-            sw[l] = i < N ? ex.rec[i] : 0.0;
-        if (Residual)
-            sk[l] = i < N ? ex.kint[i] : 0;
+        rv[j] = 0.0;
+        k_int[j] = 0;
+    }
+    if (exact && i0l < N) {
+        const double2 *r2 = reinterpret_cast<const double2 *>(ex.rec + i0l);
+#pragma unroll
+        for (int j = 0; j < kItems / 2; ++j) {
+            const double2 v = r2[j];
+            rv[2 * j] = i0l + 2 * j < N ? v.x : 0.0;
+            rv[2 * j + 1] = i0l + 2 * j + 1 < N ? v.y : 0.0;
+        }
+    }
+    if (Residual && i0l < N) {
+        const int4 *k4 = reinterpret_cast<const int4 *>(ex.kint + i0l);
+#pragma unroll
+        for (int j = 0; j < kItems / 4; ++j) {
+            const int4 v = k4[j];
+            const int q[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+                k_int[4 * j + m] = i0l + 4 * j + m < N ? q[m] : 0;
+        }
     }
     if (nsp_tile <= kExactCap && (int)threadIdx.x < nsp_tile)
         sm.sv[threadIdx.x] = ex.s_spec[(size_t)tile * kExactCap + threadIdx.x];
     __syncthreads();
-    // the tile's uniforms are loaded into registers now and written to
-    // shared memory after the records are read
+    // the tile's uniforms into shared memory, asynchronously
     const long long lo = sh_bound[0];
     const long long hi = max(sh_bound[1], lo);
     const bool staged = !Sys && (hi - lo) <= kUStage;
-    double upre[kUStage / kThreads];
     if (staged) {
-#pragma unroll
-        for (int j = 0; j < kUStage / kThreads; ++j) {
-            const long long n = lo + j * kThreads + threadIdx.x;
-            upre[j] = n < hi ? u[n] : 0.0;
-        }
+        for (int k = threadIdx.x; k < (int)(hi - lo); k += kThreads)
+            cp_async8(&sw[k], &u[lo + k]);
+        cp_async_commit();
     }
     // each particle's cumulative weight, exactly the reference's
     double Cx[kItems];
@@ -1330,28 +1423,17 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     for (int j = 0; j < kItems; ++j)
         Cx[j] = 0.0;
     if (exact) {
-        double rv[kItems];
         int nsp = 0;
 #pragma unroll
-        for (int j = 0; j < kItems; ++j) {
-            rv[j] = sw[threadIdx.x * kItems + j];
+        for (int j = 0; j < kItems; ++j)
             nsp += rv[j] < 0.0;
-        }
         int nspec;
         const int rank0 = block_excl_scan(nsp, reinterpret_cast<int *>(shl),
-                                          nspec); // ends with a barrier
+                                          nspec);
         exact_values(rv, rank0, a, sm.sv, nsp_tile > kExactCap, Cx);
-    } else {
-        __syncthreads();
     }
-    if (staged) {
-#pragma unroll
-        for (int j = 0; j < kUStage / kThreads; ++j) {
-            const long long n = lo + j * kThreads + threadIdx.x;
-            if (n < hi)
-                sw[n - lo] = upre[j];
-        }
-    }
+    if (staged)
+        cp_async_wait_all();
     __syncthreads();
 
     // counts c_i = #{n: u_n <= C_i} for this thread's particles; C_i is
@@ -1361,8 +1443,8 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     const int ilo = (int)lo, ihi = (int)hi, iNN = (int)NN, iN = (int)N;
     const int i0 = (int)base + (int)threadIdx.x * kItems;
     int cnt[kItems];
-    int k_int[kItems];
     int pos = -1;
+    long long gpos = -1;
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
         const int i = i0 + j;
@@ -1377,10 +1459,11 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
                           : ub_gallop(sw, pos, ihi - ilo, C);
             c = ilo + pos;
         } else {
-            c = (int)ub_global(u, lo, hi, C);
+            gpos = gpos < 0 ? ub_global(u, lo, hi, C)
+                            : ub_gallop_global(u, gpos, hi, C);
+            c = (int)gpos;
         }
         cnt[j] = min(max(c, ilo), i >= iN - 1 ? iNN : ihi);
-        k_int[j] = Residual ? (int)sk[threadIdx.x * kItems + j] : 0;
     }
 #pragma unroll
     for (int j = 1; j < kItems; ++j)
@@ -1925,7 +2008,7 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
             wsrc, N, ws.ctl, ws.tile_excl, ws.ex);
         k_exact_spine<W, false, true><<<1, kSpineThreads, 0, s>>>(
             wsrc, N, ws.ctl, nt, ws.ex);
-        wx = with_exact_coeff(wsrc, &ws.ctl->coeff_w);
+        wx = with_exact_coeff(wsrc, &ws.ctl->coeff_w, ws.ex.rec);
     }
     if (residual) {
         k_tile_sums<W, true><<<nt, kThreads, 0, s>>>(wx, N, ws.ctl,
