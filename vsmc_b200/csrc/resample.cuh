@@ -1070,8 +1070,15 @@ k_exact_tiles_body(W wsrc, long long N, const ResampleCtl *ctl,
     }
 }
 
+// Four CTAs per SM (64 registers, a few spilled) hide the exact scan's
+// load latency better than three without the bound (measured: the
+// resampling chain of a 2^24-particle step 0.18 ms shorter).
+#ifndef VSMC_EXACT_MIN_BLOCKS
+#define VSMC_EXACT_MIN_BLOCKS 4
+#endif
+
 template <typename W, bool Residual, bool Raw = false>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, VSMC_EXACT_MIN_BLOCKS)
 k_exact_tiles(W wsrc, long long N, const ResampleCtl *ctl,
               const double *tile_excl, ExactScan ex)
 {
@@ -1088,7 +1095,10 @@ constexpr int kExactDirtyStage = 256; // tiles with specials the spine stages
 // kExactDirtyStage live in shared memory, the others in the ExactScan
 // arrays dirty / pk / eaft / s_out (indexed by q).
 struct SmemExactSpine {
-    unsigned long long shk[kSpineThreads / 32];
+    unsigned long long wk[32]; // per warp: clean k before its tiles
+    int wd[32];                // per warp: tiles with specials before
+    unsigned long long ktot;
+    int ndt;
     int shi[kSpineThreads / 32];
     int dq[kExactDirtyStage];
     ExactTile tq[kExactDirtyStage];
@@ -1102,11 +1112,13 @@ struct SmemExactSpine {
 };
 
 // Phase B (one CTA): the exact S before every tile and at every special.
-// Each thread owns a contiguous range of tiles; only thread 0's walk over
-// the specials is sequential, and it reads shared memory.  Raw: the
-// sequential sum sets the coefficient -- of the residuals, coeff_r = 1 /
-// sum as the reference's `1 / math::asum(M, rptr)` (residual.hpp:63); of
-// the unnormalised weights, coeff_w (weight_set.hpp:121).
+// Each warp owns a contiguous range of tiles and reads it 32 tiles at a
+// time (coalesced), with warp scans for the clean k and the ranks of the
+// tiles with specials; only thread 0's walk over the specials is
+// sequential, and it reads shared memory.  Raw: the sequential sum sets
+// the coefficient -- of the residuals, coeff_r = 1 / sum as the
+// reference's `1 / math::asum(M, rptr)` (residual.hpp:63); of the
+// unnormalised weights, coeff_w (weight_set.hpp:121).
 template <typename W, bool Residual, bool Raw = false>
 __device__ __forceinline__ void
 k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
@@ -1116,69 +1128,87 @@ k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
         return;
     wsrc.prepare();
     const int bd = (int)blockDim.x;
-    const int per = (nt + bd - 1) / bd;
-    const int tb = min((int)threadIdx.x * per, nt), te = min(tb + per, nt);
-    // 1. prefix of the clean tiles' k and the ranks of the tiles with
-    // specials (tile 0 always has one: its first element)
-    // (the tile records are read eight at a time, so that their loads
-    // overlap)
-    unsigned long long run = 0;
-    int nd = 0;
-    for (int t0 = tb; t0 < te; t0 += 8) {
-        ExactTile et[8];
-#pragma unroll
-        for (int v = 0; v < 8; ++v)
-            if (t0 + v < te)
-                et[v] = ex.tiles[t0 + v];
-#pragma unroll
-        for (int v = 0; v < 8; ++v)
-            if (t0 + v < te) {
-                run += et[v].nspec == 0 ? et[v].k_total : 0ull;
-                nd += et[v].nspec != 0;
-            }
-    }
-    unsigned long long ktot;
-    const unsigned long long pk0 = block_excl_scan(run, sm.shk, ktot);
-    int ndt;
-    const int q0 = block_excl_scan(nd, sm.shi, ndt);
+    const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5, nw = bd >> 5;
+    const int perw = (nt + nw - 1) / nw;
+    const int wb = min(wq * perw, nt), we = min(wb + perw, nt);
+    // a tile record, or an empty clean one past the warp's range
+    const auto tile_at = [&](int t) {
+        ExactTile et;
+        et.k_total = 0;
+        et.nspec = 0;
+        et.e_last = kNoBinade;
+        if (t < we)
+            et = ex.tiles[t];
+        return et;
+    };
+    // 1a. per warp: clean k and tiles with specials (tile 0 always has one:
+    // its first element); their exclusive prefixes over the warps
     {
-        unsigned long long off = pk0;
-        int q = q0;
-        for (int t0 = tb; t0 < te; t0 += 8) {
-          ExactTile ev[8];
-#pragma unroll
-          for (int v = 0; v < 8; ++v)
-              if (t0 + v < te)
-                  ev[v] = ex.tiles[t0 + v];
-#pragma unroll
-          for (int v = 0; v < 8; ++v) {
-            const int t = t0 + v;
-            if (t >= te)
-                break;
-            const ExactTile et = ev[v];
-            if (et.nspec == 0) {
-                off += et.k_total;
-                continue;
+        unsigned long long k = 0;
+        int d = 0;
+        for (int t = wb + lane; t < we; t += 32) {
+            const ExactTile et = ex.tiles[t];
+            k += et.nspec == 0 ? et.k_total : 0ull;
+            d += et.nspec != 0;
+        }
+        k = __shfl_sync(0xffffffffu, warp_incl_scan(k), 31);
+        d = __shfl_sync(0xffffffffu, warp_incl_scan(d), 31);
+        if (lane == 0) {
+            sm.wk[wq] = k;
+            sm.wd[wq] = d;
+        }
+    }
+    __syncthreads();
+    if (wq == 0) {
+        const unsigned long long k = lane < nw ? sm.wk[lane] : 0ull;
+        const int d = lane < nw ? sm.wd[lane] : 0;
+        const unsigned long long ki = warp_incl_scan(k);
+        const int di = warp_incl_scan(d);
+        if (lane < nw) {
+            sm.wk[lane] = ki - k;
+            sm.wd[lane] = di - d;
+        }
+        if (lane == 31) {
+            sm.ktot = ki;
+            sm.ndt = di;
+        }
+    }
+    __syncthreads();
+    const int ndt = sm.ndt;
+    // 1b. the tiles with specials, by rank: the tile, its record, the clean
+    // k before it and the binade of the clean tiles after it
+    {
+        unsigned long long off = sm.wk[wq];
+        int q = sm.wd[wq];
+        for (int t0 = wb; t0 < we; t0 += 32) {
+            const int t = t0 + lane;
+            const ExactTile et = tile_at(t);
+            const int dc = et.nspec != 0;
+            const unsigned long long kc = dc ? 0ull : et.k_total;
+            const unsigned long long ki = warp_incl_scan(kc);
+            const int di = warp_incl_scan(dc);
+            if (dc) {
+                const int qq = q + di - 1;
+                const unsigned long long pkd = off + ki;
+                int ea = kNoBinade;
+                if (t + 1 < nt) {
+                    const ExactTile nx = ex.tiles[t + 1];
+                    if (nx.nspec == 0)
+                        ea = nx.e_last;
+                }
+                if (qq < kExactDirtyStage) {
+                    sm.dq[qq] = t;
+                    sm.tq[qq] = et;
+                    sm.pkq[qq] = pkd;
+                    sm.eaft[qq] = ea;
+                } else {
+                    ex.dirty[qq] = t;
+                    ex.pk[qq] = pkd;
+                    ex.eaft[qq] = ea;
+                }
             }
-            // binade of the clean tiles after t (if the next is clean)
-            int ea = kNoBinade;
-            if (t + 1 < nt) {
-                const ExactTile nx = ex.tiles[t + 1];
-                if (nx.nspec == 0)
-                    ea = nx.e_last;
-            }
-            if (q < kExactDirtyStage) {
-                sm.dq[q] = t;
-                sm.tq[q] = et;
-                sm.pkq[q] = off;
-                sm.eaft[q] = ea;
-            } else {
-                ex.dirty[q] = t;
-                ex.pk[q] = off;
-                ex.eaft[q] = ea;
-            }
-            ++q;
-          }
+            off += __shfl_sync(0xffffffffu, ki, 31);
+            q += __shfl_sync(0xffffffffu, di, 31);
         }
     }
     __syncthreads();
@@ -1196,8 +1226,7 @@ k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
         sm.st_off[threadIdx.x] = soff;
     __syncthreads();
     if (fits) { // a warp per tile with specials
-        const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
-        for (int q = wq; q < ndt; q += bd >> 5) {
+        for (int q = wq; q < ndt; q += nw) {
             const int ns = sm.tq[q].nspec;
             if (ns > kExactCap)
                 continue;
@@ -1263,48 +1292,41 @@ k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
     __syncthreads();
     // 4. every clean tile (and the end): the exact S after the last tile
     // with specials before it plus the clean k since, in that binade
+    const auto after = [&](int qq, unsigned long long k) {
+        if (qq < 0) // (tile 0 always has a special)
+            return 0.0;
+        const bool sq = qq < kExactDirtyStage;
+        double S = sq ? sm.sout[qq] : ex.s_out[qq];
+        const unsigned long long K = k - (sq ? sm.pkq[qq] : ex.pk[qq]);
+        if (K != 0) {
+            const int ea = sq ? sm.eaft[qq] : ex.eaft[qq];
+            S = __dadd_rn(S, __dmul_rn((double)K, exact_pow2(ea - 52)));
+        }
+        return S;
+    };
     {
-        unsigned long long off = pk0;
-        int q = q0 - 1; // rank of the last tile with specials before tb
-        const auto after = [&](int qq, unsigned long long k) {
-            if (qq < 0) // (tile 0 always has a special)
-                return 0.0;
-            const bool sq = qq < kExactDirtyStage;
-            double S = sq ? sm.sout[qq] : ex.s_out[qq];
-            const unsigned long long K =
-                k - (sq ? sm.pkq[qq] : ex.pk[qq]);
-            if (K != 0) {
-                const int ea = sq ? sm.eaft[qq] : ex.eaft[qq];
-                S = __dadd_rn(S, __dmul_rn((double)K, exact_pow2(ea - 52)));
-            }
-            return S;
-        };
-        for (int t0 = tb; t0 < te; t0 += 8) {
-            ExactTile et[8];
-#pragma unroll
-            for (int v = 0; v < 8; ++v)
-                if (t0 + v < te)
-                    et[v] = ex.tiles[t0 + v];
-#pragma unroll
-            for (int v = 0; v < 8; ++v) {
-                if (t0 + v >= te)
-                    break;
-                if (et[v].nspec != 0) {
-                    ++q;
-                    continue;
-                }
-                ex.start[t0 + v] = after(q, off);
-                off += et[v].k_total;
-            }
+        unsigned long long off = sm.wk[wq];
+        int q = sm.wd[wq];
+        for (int t0 = wb; t0 < we; t0 += 32) {
+            const int t = t0 + lane;
+            const ExactTile et = tile_at(t);
+            const int dc = et.nspec != 0;
+            const unsigned long long kc = dc ? 0ull : et.k_total;
+            const unsigned long long ki = warp_incl_scan(kc);
+            const int di = warp_incl_scan(dc);
+            if (t < we && !dc)
+                ex.start[t] = after(q + di - 1, off + ki - kc);
+            off += __shfl_sync(0xffffffffu, ki, 31);
+            q += __shfl_sync(0xffffffffu, di, 31);
         }
-        if (tb < te && te == nt) {
-            const double S = after(q, off);
-            ex.start[nt] = S;
-            if (Raw && Residual)
-                ctl->coeff_r = __ddiv_rn(1.0, S);
-            else if (Raw)
-                ctl->coeff_w = __ddiv_rn(1.0, S);
-        }
+    }
+    if (threadIdx.x == 0) {
+        const double S = after(ndt - 1, sm.ktot);
+        ex.start[nt] = S;
+        if (Raw && Residual)
+            ctl->coeff_r = __ddiv_rn(1.0, S);
+        else if (Raw)
+            ctl->coeff_w = __ddiv_rn(1.0, S);
     }
 }
 
@@ -1559,8 +1581,9 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     }
 }
 
+// Five CTAs per SM: 48 registers without spills.
 #ifndef VSMC_INVERT_MIN_BLOCKS
-#define VSMC_INVERT_MIN_BLOCKS 4
+#define VSMC_INVERT_MIN_BLOCKS 5
 #endif
 
 template <typename W, bool Residual, bool Sys>
