@@ -123,16 +123,15 @@ __global__ void __launch_bounds__(kMoveThreads, MinBlocks * 256 / kMoveThreads)
 kb_move(const BatchSlot *slots, const TileRef *map, CVParam p)
 {
     __shared__ double sh_w[7 * kMoveWarps];
-    extern __shared__ double2 pts[]; // kPolarSmemBytes
     const TileRef r = map[blockIdx.x];
     const BatchSlot &b = slots[r.slot];
     const MoveArgs<Real> a = batch_move_args<Real>(b, p);
     if (a.iter == 0) {
         const MoveStep<Real> ms = move_step<Real, true>(a);
-        cv_move_tile<Real, true>(a, ms, r.tile, sh_w, pts);
+        cv_move_tile<Real, true>(a, ms, r.tile, sh_w);
     } else {
         const MoveStep<Real> ms = move_step<Real, false>(a);
-        cv_move_tile<Real, false>(a, ms, r.tile, sh_w, pts);
+        cv_move_tile<Real, false>(a, ms, r.tile, sh_w);
     }
 }
 
@@ -349,7 +348,6 @@ union SmemBlockPhase {
 
 template <bool Residual>
 struct SmemBlock {
-    double2 pts[2 * kTile]; // the move's polar points
     SmemBlockPhase<Residual> ph;
     double agg[kBlockMaxTiles];
     double sh_w[2][7 * kMoveWarps];
@@ -392,13 +390,12 @@ kb_block_run(BatchSlot *slots, const BlockItem *items, int n, int *queue,
                 if (a.iter == 0) {
                     const MoveStep<Real> ms = move_step<Real, true>(a);
                     for (int tile = 0; tile < nt; ++tile, buf ^= 1)
-                        cv_move_tile<Real, true>(a, ms, tile, sm.sh_w[buf],
-                                                 sm.pts);
+                        cv_move_tile<Real, true>(a, ms, tile, sm.sh_w[buf]);
                 } else {
                     const MoveStep<Real> ms = move_step<Real, false>(a);
                     for (int tile = 0; tile < nt; ++tile, buf ^= 1)
-                        cv_move_tile<Real, false>(a, ms, tile, sm.sh_w[buf],
-                                                  sm.pts);
+                        cv_move_tile<Real, false>(a, ms, tile,
+                                                  sm.sh_w[buf]);
                 }
             }
             __syncthreads();
@@ -958,15 +955,15 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
     const int32_t *work = b->d_work;
     switch (b->tune_move) {
     case 2:
-        kb_move<Real, 2><<<nt, kMoveThreads, kPolarSmemBytes, s>>>(
+        kb_move<Real, 2><<<nt, kMoveThreads, 0, s>>>(
             sl, map, b->bc.p);
         break;
     case 4:
-        kb_move<Real, 4><<<nt, kMoveThreads, kPolarSmemBytes, s>>>(
+        kb_move<Real, 4><<<nt, kMoveThreads, 0, s>>>(
             sl, map, b->bc.p);
         break;
     default:
-        kb_move<Real, 3><<<nt, kMoveThreads, kPolarSmemBytes, s>>>(
+        kb_move<Real, 3><<<nt, kMoveThreads, 0, s>>>(
             sl, map, b->bc.p);
         break;
     }
@@ -1176,12 +1173,6 @@ int vsmc_cuda_cv_batch_create(const vsmc_cuda_cv_config *model,
     if (b == nullptr)
         return VSMC_CUDA_ENOMEM;
     b->model = *model;
-    set_move_smem_attribute(kb_move<double, 2>);
-    set_move_smem_attribute(kb_move<double, 3>);
-    set_move_smem_attribute(kb_move<double, 4>);
-    set_move_smem_attribute(kb_move<float, 2>);
-    set_move_smem_attribute(kb_move<float, 3>);
-    set_move_smem_attribute(kb_move<float, 4>);
     b->bc.p = cv_param(*model);
     b->bc.threshold = model->threshold;
     b->bc.residual = is_residual(model->scheme);

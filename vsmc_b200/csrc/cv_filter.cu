@@ -169,11 +169,9 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
         cudaEventRecord(ev[0], s);
     }
     if (init)
-        k_cv_move<Real, true>
-            <<<f->move_grid, kMoveThreads, kPolarSmemBytes, s>>>(a);
+        k_cv_move<Real, true><<<f->move_grid, kMoveThreads, 0, s>>>(a);
     else
-        k_cv_move<Real, false>
-            <<<f->move_grid, kMoveThreads, kPolarSmemBytes, s>>>(a);
+        k_cv_move<Real, false><<<f->move_grid, kMoveThreads, 0, s>>>(a);
     if (ev)
         cudaEventRecord(ev[1], s);
     f->cur = dst;
@@ -414,7 +412,6 @@ int vsmc_cuda_cv_create(const vsmc_cuda_cv_config *cfg, void *stream,
     cudaFuncSetAttribute(k_cv_finalize,
                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                          kFinalSmemTiles * (int)sizeof(double));
-    set_move_smem_attributes();
     // one CTA per tile: the block scheduler hands tiles to SMs as they
     // free, which balances the rejection loops' uneven cost better than a
     // persistent grid striding over tiles (measured 5% faster at 2^24)

@@ -82,12 +82,23 @@ __device__ __forceinline__ PhiloxStream particle_stream(uint32_t iter,
 }
 
 // The two accepted polar points of one particle's step (libstdc++'s two
-// calls of the polar loop), drawn by polar_points_tile.  r2 = x^2 + y^2 is
-// recomputed with the same two products and sum, so it is the value the
-// acceptance test saw.
+// calls of the polar loop), from the particle's own Philox stream
+// (polar_two).  r2 = x^2 + y^2 is recomputed with the same two products and
+// sum, so it is the value the acceptance test saw.
 struct PolarPair {
     double x1, y1, x2, y2;
 };
+
+__device__ __forceinline__ PolarPair polar_pair_draw(uint32_t iter,
+                                                     uint32_t id,
+                                                     uint32_t stream,
+                                                     uint32_t k0, uint32_t k1)
+{
+    PolarPair pp;
+    double q1, q2;
+    polar_two(iter, id, stream, k0, k1, pp.x1, pp.y1, q1, pp.x2, pp.y2, q2);
+    return pp;
+}
 
 __device__ __forceinline__ double polar_r2(double x, double y)
 {
@@ -216,79 +227,14 @@ constexpr int kMoveThreads = 256;                 // threads of a move CTA
 constexpr int kMoveItems = kTile / kMoveThreads; // particles per thread
 constexpr int kMoveWarps = kMoveThreads / 32;
 
-// Shared memory a move CTA needs for its polar points: two (x, y) pairs
-// for each of its kTile particles (64 KiB).
-constexpr size_t kPolarSmemBytes = (size_t)kTile * 2 * sizeof(double2);
-
-// Phase 1 of a move tile: the polar points of the thread's kMoveItems
-// particles.  A particle's points come from its own Philox4x32-10 stream
-// (counter {block, step, id, stream}, block = 1, 2, ...), one block per
-// polar attempt, and the polar method (libstdc++ normal_distribution)
-// keeps the first two attempts with 0 < x^2 + y^2 <= 1.  The thread walks
-// its particles one after another through a single loop of one block per
-// iteration, so a warp runs for the largest total number of attempts of a
-// lane (about 25 for 8 particles, 2.55 expected per particle) instead of
-// paying the slowest lane's rejection tail once per particle (about 4.8
-// blocks per particle).  Each particle's points are the same as the
-// sequential loop's, in stream order.  `pts` is the thread's slice:
-// slot (2 j + k) * kMoveThreads + threadIdx.x holds point k of the thread's
-// j-th particle; only this thread reads it back, so no barrier is needed.
-template <int V>
-__device__ __forceinline__ void polar_points_tile(uint32_t iter,
-                                                  uint32_t stream,
-                                                  uint32_t k0, uint32_t k1,
-                                                  long long base, long long N,
-                                                  double2 *pts)
-{
-    // the thread's j-th particle: pass v = j / V, element e = j % V
-    auto pid = [&](int j) {
-        return base + ((long long)(j / V) * kMoveThreads + threadIdx.x) * V +
-               (j % V);
-    };
-    long long id = pid(0);
-    if (id >= N)
-        return;
-    PhiloxStream s;
-    s.ctr = make_uint4(0u, iter, (uint32_t)id, stream);
-    s.k0 = k0;
-    s.k1 = k1;
-    int j = 0, k = 0;
-#pragma unroll 1
-    while (true) {
-        double x, y, r2;
-        polar_point(s.next_block(), x, y, r2);
-        if (polar_ok(r2)) {
-            pts[(2 * j + k) * kMoveThreads + threadIdx.x] = make_double2(x, y);
-            if (++k == 2) {
-                k = 0;
-                if (++j == kMoveItems)
-                    break;
-                id = pid(j);
-                if (id >= N)
-                    break;
-                s.ctr = make_uint4(0u, iter, (uint32_t)id, stream);
-            }
-        }
-    }
-}
-
-__device__ __forceinline__ PolarPair polar_pair(const double2 *pts, int j)
-{
-    const double2 a = pts[(2 * j) * kMoveThreads + threadIdx.x];
-    const double2 b = pts[(2 * j + 1) * kMoveThreads + threadIdx.x];
-    return PolarPair{a.x, a.y, b.x, b.y};
-}
-
 // One tile of kTile particles: load (gather), move, likelihood, log-weight
 // update and the tile's online log-sum-exp statistics.  `sh_w` holds
 // 7 x kMoveWarps warp partials; a CTA alternates two such buffers so that
-// one barrier per tile suffices.  `pts` is kPolarSmemBytes of shared memory
-// for the polar points (phase 1), which the move (phase 2) consumes.
+// one barrier per tile suffices.
 template <typename Real, bool Init>
 __device__ __forceinline__ void cv_move_tile(const MoveArgs<Real> &a,
                                              const MoveStep<Real> &ms,
-                                             int tile, double *sh_w,
-                                             double2 *pts)
+                                             int tile, double *sh_w)
 {
     constexpr int V = Vec<Real>::n;
     constexpr int NV = kMoveItems / V;
@@ -300,7 +246,6 @@ __device__ __forceinline__ void cv_move_tile(const MoveArgs<Real> &a,
     const long long N = a.N;
     {
         const long long base = (long long)tile * kTile;
-        polar_points_tile<V>(a.iter, a.stream, a.k0, a.k1, base, N, pts);
         LseRef acc;
         acc.init();
         double gx = 0.0, gy = 0.0;
@@ -353,8 +298,11 @@ __device__ __forceinline__ void cv_move_tile(const MoveArgs<Real> &a,
             for (int e = 0; e < V; ++e) {
                 const long long i = p0 + e;
                 if (i < N) {
-                    cv_particle<Init>(a.p, polar_pair(pts, v * V + e), s[0][e],
-                                      s[1][e], s[2][e], s[3][e], shx, shy);
+                    cv_particle<Init>(
+                        a.p,
+                        polar_pair_draw(a.iter, (uint32_t)i, a.stream, a.k0,
+                                        a.k1),
+                        s[0][e], s[1][e], s[2][e], s[3][e], shx, shy);
                     const Real inc = cv_loglik(a.p, s[0][e], s[1][e], ox, oy);
                     // lw += -max (normalize_log_weight), then += inc
                     lwn[e] = Init ? inc : (lwv[e] - mprev) + inc;
@@ -401,41 +349,12 @@ k_cv_move(MoveArgs<Real> a)
 {
     // double-buffered warp partials: one barrier per tile
     __shared__ double sh_w[2][7 * kMoveWarps];
-    extern __shared__ double2 pts[]; // kPolarSmemBytes
     const MoveStep<Real> ms = move_step<Real, Init>(a);
     int buf = 0;
     for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        cv_move_tile<Real, Init>(a, ms, tile, sh_w[buf], pts);
+        cv_move_tile<Real, Init>(a, ms, tile, sh_w[buf]);
         buf ^= 1;
     }
-}
-
-// The move kernels take kPolarSmemBytes of dynamic shared memory (above
-// the 48 KiB default) and prefer the shared-memory carve-out that fits
-// three such CTAs per SM; set once per device before their first launch.
-template <typename K>
-inline cudaError_t set_move_smem_attribute(K kernel)
-{
-    cudaError_t e = cudaFuncSetAttribute(
-        kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        (int)kPolarSmemBytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(kernel,
-                                 cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared);
-    return e;
-}
-
-inline cudaError_t set_move_smem_attributes()
-{
-    cudaError_t e = set_move_smem_attribute(k_cv_move<double, true>);
-    if (e == cudaSuccess)
-        e = set_move_smem_attribute(k_cv_move<double, false>);
-    if (e == cudaSuccess)
-        e = set_move_smem_attribute(k_cv_move<float, true>);
-    if (e == cudaSuccess)
-        e = set_move_smem_attribute(k_cv_move<float, false>);
-    return e;
 }
 
 struct FinalizeArgs {
