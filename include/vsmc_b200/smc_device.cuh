@@ -19,6 +19,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "fastmath.cuh"
+
 #if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ != 1000)
 #error "libvsmc_cuda is written for sm_100a (B200) only"
 #endif
@@ -208,7 +210,7 @@ struct TileStats {
     double m, s1, s2, sx, sy, gx, gy, pad;
 };
 
-__device__ __forceinline__ double lse_exp(double v) { return exp(v); }
+__device__ __forceinline__ double lse_exp(double v) { return fm::fm_exp(v); }
 __device__ __forceinline__ double lse_exp(float v) { return (double)expf(v); }
 
 // Per-thread weight statistics against a lazy reference: the first finite
@@ -253,7 +255,7 @@ __device__ __forceinline__ void lse_add(LseRef &a, Real lw, Real x, Real y)
     if (a.ref == -INFINITY) {
         a.ref = l;
     } else if (l - a.ref > LazyBound<Real>::v) {
-        const double f = exp(a.ref - l);
+        const double f = fm::fm_exp(a.ref - l);
         a.s1 *= f;
         a.s2 *= f * f;
         a.sx *= f;
@@ -270,7 +272,7 @@ __device__ __forceinline__ void lse_add(LseRef &a, Real lw, Real x, Real y)
 // Rescale a thread's sums to the common maximum M: exp(ref - M) <= 1.
 __device__ __forceinline__ void lse_rescale(LseRef &a, double M)
 {
-    const double f = a.ref == -INFINITY ? 0.0 : exp(a.ref - M);
+    const double f = a.ref == -INFINITY ? 0.0 : fm::fm_exp(a.ref - M);
     a.s1 *= f;
     a.s2 *= f * f;
     a.sx *= f;

@@ -197,6 +197,14 @@ int vsmc_cuda_resample_noalloc(int scheme, uint64_t N, const double *weight,
 int vsmc_cuda_copy_f64(uint64_t N, uint32_t dim, const double *src,
                        double *dst, const int32_t *copy_from, void *stream);
 
+/* The library's FP64 natural logarithm (fn 0) and exponential (fn 1) --
+ * the table-driven functions its kernels evaluate the move, the weights and
+ * the sorted U01 sequence with (include/vsmc_b200/fastmath.cuh) -- on n
+ * device values: out[i] = f(in[i]).  For checking them against other
+ * implementations. */
+int vsmc_cuda_math_eval(int fn, uint64_t n, const double *in, double *out,
+                        void *stream);
+
 /* ------------------------------------------------ CV Student-t filter ---- */
 
 /* The constant-velocity Student-t bootstrap filter of example/pf

@@ -88,6 +88,7 @@ def lib():
     L.vsmc_cuda_resample.argtypes = [i32, u64, vp, vp, u64, C.POINTER(ThreefryState),
                                      vp, vp, vp, C.c_size_t, vp]
     L.vsmc_cuda_copy_f64.argtypes = [u64, C.c_uint32, vp, vp, vp, vp]
+    L.vsmc_cuda_math_eval.argtypes = [C.c_int, u64, vp, vp, vp]
     L.vsmc_cuda_resample_mn_workspace_size.restype = C.c_size_t
     L.vsmc_cuda_resample_mn_workspace_size.argtypes = [u64, u64]
     L.vsmc_cuda_resample_mn.argtypes = [i32, u64, u64, vp, vp, u64,
@@ -284,6 +285,12 @@ def resample_noalloc(scheme, N, weight_ptr, rng: ThreefryState, rep_ptr, cf_ptr,
 def copy_f64(N, dim, src_ptr, dst_ptr, cf_ptr, stream=None):
     check(lib().vsmc_cuda_copy_f64(N, dim, src_ptr, dst_ptr, cf_ptr, stream),
           "vsmc_cuda_copy_f64")
+
+
+def math_eval(fn, n, in_ptr, out_ptr, stream=None) -> None:
+    """The library's FP64 log (fn 0) or exp (fn 1) of n device doubles."""
+    check(lib().vsmc_cuda_math_eval(fn, n, in_ptr, out_ptr, stream),
+          "vsmc_cuda_math_eval")
 
 
 # -------------------------------------------------------- CV filter -------

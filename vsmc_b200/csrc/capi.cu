@@ -199,6 +199,14 @@ __global__ void k_copy_f64(long long N, unsigned dim, const double *src,
         dst[(long long)d * N + i] = src[(long long)d * N + c];
 }
 
+static __global__ void k_math_eval(int fn, long long n, const double *in,
+                                   double *out)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = fn == 0 ? fm::fm_log(in[i]) : fm::fm_exp(in[i]);
+}
+
 } // namespace vsmc_b200
 
 using namespace vsmc_b200;
@@ -550,6 +558,22 @@ int vsmc_cuda_copy_f64(uint64_t N, uint32_t dim, const double *src,
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? VSMC_CUDA_OK
                             : cuda_status(e, "vsmc_cuda_copy_f64");
+}
+
+int vsmc_cuda_math_eval(int fn, uint64_t n, const double *in, double *out,
+                        void *stream)
+{
+    if ((fn != 0 && fn != 1) || n == 0 || in == nullptr || out == nullptr) {
+        set_last_error("vsmc_cuda_math_eval: invalid arguments");
+        return VSMC_CUDA_EINVAL;
+    }
+    const long long blocks = ((long long)n + 255) / 256;
+    k_math_eval<<<(unsigned)(blocks < 4736 ? blocks : 4736), 256, 0,
+                  static_cast<cudaStream_t>(stream)>>>(fn, (long long)n, in,
+                                                       out);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VSMC_CUDA_OK
+                            : cuda_status(e, "vsmc_cuda_math_eval");
 }
 
 int vsmc_cuda_device_alloc(size_t bytes, void **ptr)

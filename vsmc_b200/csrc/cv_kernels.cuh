@@ -146,7 +146,7 @@ __device__ __forceinline__ double cv_loglik(const CVParam &p, double x,
     const double lx = p.scale * (x - ox);
     const double ly = p.scale * (y - oy);
     const double a = lx * lx * p.inv_nu, b = ly * ly * p.inv_nu;
-    return p.coef * log((1.0 + a) * (1.0 + b));
+    return p.coef * fm::fm_log((1.0 + a) * (1.0 + b));
 }
 
 // Mixed form: the same stream consumption; float transforms and state.  The
@@ -485,7 +485,7 @@ __device__ __forceinline__ void k_cv_finalize_body(const FinalizeArgs &a,
             const int t = t0 + k * bd;
             if (t < nt) {
                 const TileStats &ts = tb[k];
-                const double f = ts.m == -INFINITY ? 0.0 : exp(ts.m - M);
+                const double f = ts.m == -INFINITY ? 0.0 : fm::fm_exp(ts.m - M);
                 const double s1 = ts.s1 * f;
                 share[t] = s1;
                 v[0] += s1;

@@ -176,7 +176,7 @@ template <>
 __device__ __forceinline__ double
 WeightsFromLog<double>::unnorm(long long i) const
 {
-    return raw != nullptr ? raw[i] : exp(__dadd_rn(lw[i], -M));
+    return raw != nullptr ? raw[i] : fm::fm_exp(__dadd_rn(lw[i], -M));
 }
 
 template <>
@@ -601,7 +601,8 @@ __device__ __forceinline__ void sorted_terms8(const EngineRef &eng,
     for (int j = 0; j < 8; ++j) {
         const long long n = n0 + j;
         const double U = canonical_u64(w[j]);
-        t[j] = n < NN ? __ddiv_rn(log(__dadd_rn(1.0, -U)), (double)(NN - n))
+        t[j] = n < NN ? __ddiv_rn(fm::fm_log(__dadd_rn(1.0, -U)),
+                                  (double)(NN - n))
                       : 0.0;
     }
 }
@@ -722,7 +723,7 @@ k_sorted_uniforms_body(EngineRef eng, const ResampleCtl *ctl,
     const double a = tile_excl[bid];
     const double b = tile_excl[bid + 1];
     // carry: the previous tile ends exactly at lmax = a
-    const double umax = bid > 0 ? __dadd_rn(1.0, -exp(a)) : -INFINITY;
+    const double umax = bid > 0 ? __dadd_rn(1.0, -fm::fm_exp(a)) : -INFINITY;
     double uv[kItems];
     double tmax = -INFINITY;
 #pragma unroll
@@ -731,7 +732,7 @@ k_sorted_uniforms_body(EngineRef eng, const ResampleCtl *ctl,
         double lmax = fmax(__dadd_rn(a, pre), b); // lmax is non-increasing
         if (n0 + j == last)
             lmax = b;
-        uv[j] = __dadd_rn(1.0, -exp(lmax));
+        uv[j] = __dadd_rn(1.0, -fm::fm_exp(lmax));
         tmax = fmax(tmax, uv[j]);
     }
     // block exclusive max-scan (max is exact, so any order gives the same

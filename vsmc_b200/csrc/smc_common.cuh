@@ -78,7 +78,7 @@ __device__ __forceinline__ void polar_two(uint32_t iter, uint32_t id,
 // caches x*mult.
 __device__ __forceinline__ double polar_mult_f64(double r2)
 {
-    return __dsqrt_rn(__ddiv_rn(__dmul_rn(-2.0, log(r2)), r2));
+    return __dsqrt_rn(__ddiv_rn(__dmul_rn(-2.0, fm::fm_log(r2)), r2));
 }
 
 __device__ __forceinline__ float polar_mult_f32(double r2)
