@@ -362,3 +362,24 @@ def test_tie_heavy_weights_bit_exact(capi, sch):
     assert words == ref_words
     assert np.array_equal(rep, ref_rep)
     assert np.array_equal(cf, ref_cf)
+
+
+@pytest.mark.parametrize("sch", LOG_EXP_SCHEMES)
+def test_benchmark_size_device_sequence(capi, sch):
+    """The sorted U01 sequence drawn on the device at 2^24: its lmax is the
+    reference's sequential sum exactly (exact scan of the negated terms), so
+    replication can differ from the oracle's only where the device's log or
+    exp rounds differently from glibc's and a uniform lies within that
+    rounding of a cumulative weight."""
+    N = 1 << 24
+    rng = np.random.default_rng(4242 + sch)
+    lw = rng.normal(size=N) * 2.0
+    w = np.exp(lw - lw.max())
+    w /= w.sum()
+    ref_rep, ref_cf, ref_words, _ = O.resample(sch, w, 103, 7, want_uniforms=True)
+    rep, cf, words = gpu_resample(capi, sch, w, 103, 7)
+    mism = int(np.count_nonzero(rep != ref_rep))
+    print(f"scheme {sch} N={N}: {mism} replication counts differ from the oracle")
+    assert words == ref_words
+    assert rep.sum() == N
+    assert mism <= 16

@@ -236,8 +236,30 @@ kb_sorted_uniforms(const BatchSlot *slots, const TileRef *map)
     __shared__ SmemSortedUniforms sm;
     const TileRef r = map[blockIdx.x];
     const BatchSlot &b = slots[r.slot];
-    k_sorted_uniforms_body(b.eng, b.rws.ctl, b.rws.u_tile_excl, b.rws.u,
-                           b.rws.bins, r.tile, sm);
+    k_sorted_uniforms_body(b.rws.ctl, b.rws.exu, b.rws.u, b.rws.bins, r.tile,
+                           sm);
+}
+
+// The exact lmax of a slot's sorted sequence (exact_scan.cuh over the
+// negated terms): per tile, then per slot.
+static __global__ void __launch_bounds__(kThreads, VSMC_EXACT_MIN_BLOCKS)
+kb_exact_terms_tiles(const BatchSlot *slots, const TileRef *map)
+{
+    __shared__ SmemExactTiles<false> sm;
+    const TileRef r = map[blockIdx.x];
+    const BatchSlot &b = slots[r.slot];
+    k_exact_tiles_body<TermsNeg, false>(TermsNeg{b.rws.u, 0}, b.N, b.rws.ctl,
+                                        b.rws.u_tile_excl, b.rws.exu, r.tile,
+                                        sm);
+}
+
+static __global__ void __launch_bounds__(kSpineThreads)
+kb_exact_terms_spine(const BatchSlot *slots, const int32_t *work)
+{
+    __shared__ SmemExactSpine sm;
+    const BatchSlot &b = slots[work[blockIdx.x]];
+    k_exact_spine_body<TermsNeg, false>(TermsNeg{b.rws.u, 0}, b.N, b.rws.ctl,
+                                        b.ntiles, b.rws.exu, sm);
 }
 
 template <typename Real, bool Residual, bool Sys>
@@ -470,9 +492,18 @@ kb_block_run(BatchSlot *slots, const BlockItem *items, int n, int *queue,
                 k_sorted_spine_body(b.rws.u_tile_sum, b.rws.u_tile_excl,
                                     b.rws.ctl, 0, sm.ph.sp);
                 __syncthreads();
+                const TermsNeg tn{b.rws.u, 0};
                 for (int tile = 0; tile < nt; ++tile) {
-                    k_sorted_uniforms_body(b.eng, b.rws.ctl,
-                                           b.rws.u_tile_excl, b.rws.u,
+                    k_exact_tiles_body<TermsNeg, false>(
+                        tn, b.N, b.rws.ctl, b.rws.u_tile_excl, b.rws.exu,
+                        tile, sm.ph.ext0);
+                    __syncthreads();
+                }
+                k_exact_spine_body<TermsNeg, false>(tn, b.N, b.rws.ctl, nt,
+                                                    b.rws.exu, sm.ph.exs);
+                __syncthreads();
+                for (int tile = 0; tile < nt; ++tile) {
+                    k_sorted_uniforms_body(b.rws.ctl, b.rws.exu, b.rws.u,
                                            b.rws.bins, tile, sm.ph.su);
                     __syncthreads();
                 }
@@ -995,8 +1026,10 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
     } else if (!sys) {
         kb_sorted_tile_sums<<<nt, kThreads, 0, s>>>(sl, map);
         kb_sorted_spine<<<n, kSpineThreads, 0, s>>>(sl, work);
+        kb_exact_terms_tiles<<<nt, kThreads, 0, s>>>(sl, map);
+        kb_exact_terms_spine<<<n, kSpineThreads, 0, s>>>(sl, work);
         kb_sorted_uniforms<<<nt, kThreads, 0, s>>>(sl, map);
-        launches += 3;
+        launches += 5;
     }
     if (residual) {
         kb_exact_tiles<Real, true, true><<<nt, kThreads, 0, s>>>(sl, map);

@@ -112,7 +112,7 @@ void enqueue_sequence(vsmc_cuda_cv_filter *f)
     launch_spec_sorted((long long)f->cfg.N, f->eng, f->rws, f->side);
     cudaEventRecord(f->ev_seq, f->side);
     f->seq_pending = true;
-    f->launches += 4;
+    f->launches += 6;
 }
 
 // The filter's stream waits for the side stream's last sequence (after a
@@ -232,7 +232,7 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
         launch_resample_core(c.scheme, w, N, f->eng, f->rws, nullptr, 0,
                              /*spine_done=*/true, nullptr, f->copy_from, s,
                              /*sorted_ready=*/true);
-        f->launches -= 3; // the sequence's launches are counted on the side
+        f->launches -= 5; // the sequence's launches are counted on the side
         enqueue_sequence(f); // for the next resampling
     } else {
         launch_resample_core(c.scheme, w, N, f->eng, f->rws, nullptr, 0,

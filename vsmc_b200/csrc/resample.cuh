@@ -118,6 +118,11 @@ __device__ __forceinline__ void bin_window(const int32_t *L, int kb,
     hi = L[k + 1];
 }
 
+constexpr int resample_ntiles(long long N)
+{
+    return (int)((N + kTile - 1) / kTile);
+}
+
 // Weight sources --------------------------------------------------------
 // Normalised weights given in memory (generic C ABI).
 struct WeightsGiven {
@@ -135,6 +140,16 @@ struct WeightsGiven {
     // the approximate spine's scale relative to these weights'
     __device__ __forceinline__ double spine_ratio() const { return 1.0; }
     __device__ __forceinline__ double spine_unnorm() const { return 1.0; }
+    // whether the resampling runs, and the scanned length
+    __device__ __forceinline__ bool active(const ResampleCtl *ctl) const
+    {
+        return ctl->active != 0;
+    }
+    __device__ __forceinline__ long long length(const ResampleCtl *,
+                                                long long N) const
+    {
+        return N;
+    }
 };
 
 // Weights of a filter: w_i = exp(lw_i - M) * coeff, i.e. the reference's
@@ -170,6 +185,15 @@ struct WeightsFromLog {
     {
         return stats[1];
     }
+    __device__ __forceinline__ bool active(const ResampleCtl *ctl) const
+    {
+        return ctl->active != 0;
+    }
+    __device__ __forceinline__ long long length(const ResampleCtl *,
+                                                long long N) const
+    {
+        return N;
+    }
 };
 
 template <>
@@ -192,6 +216,38 @@ WeightsFromLog<float>::unnorm(long long i) const
 {
     return static_cast<double>(expf(lw[i] - static_cast<float>(M)));
 }
+
+// The sorted U01 sequence's negated terms -log(1 - U_n) / (NN - n) >= 0,
+// which pass 1 stores in u[]: their exact sequential sum is the reference's
+// -lmax_n (u01.hpp:185-186).  spec_N > 0: the speculative Multinomial
+// sequence of spec_N uniforms (sorted_run).
+struct TermsNeg {
+    static constexpr bool kExactNorm = false;
+    const double *u;
+    long long spec_N;
+    __device__ __forceinline__ void prepare() {}
+    __device__ __forceinline__ double operator()(long long i) const
+    {
+        return -u[i];
+    }
+    __device__ __forceinline__ double unnorm(long long i) const
+    {
+        return -u[i];
+    }
+    // the spine of the sorted sequence sums the terms themselves
+    __device__ __forceinline__ double spine_ratio() const { return -1.0; }
+    __device__ __forceinline__ double spine_unnorm() const { return -1.0; }
+    __device__ __forceinline__ bool active(const ResampleCtl *ctl) const
+    {
+        return spec_N > 0 ? ctl->spec_offset != ctl->offset
+                          : ctl->active != 0;
+    }
+    __device__ __forceinline__ long long length(const ResampleCtl *ctl,
+                                                long long) const
+    {
+        return spec_N > 0 ? spec_N : ctl->NN;
+    }
+};
 
 // The weight source with the exact normalisation coefficient (held in the
 // control block once the normalisation pass has run) and the unnormalised
@@ -267,6 +323,8 @@ struct SmemSortedSums {
 struct SmemSortedUniforms {
     double sh[kThreads / 32];
     double shm[kThreads];
+    int shi[kThreads / 32];
+    double sv[kExactCap]; // exact -lmax at the tile's specials
 };
 // Uniforms staged in shared memory per tile: twice the expected count, so
 // that only a tile holding more than twice its share searches global memory.
@@ -694,45 +752,56 @@ k_sorted_spine(const double *tile_sum, double *tile_excl,
     k_sorted_spine_body(tile_sum, tile_excl, ctl, blockIdx.x, sm);
 }
 
+// Pass 2: u_n = 1 - exp(lmax_n) with lmax_n the reference's sequential sum
+// exactly, from the exact scan of the negated terms (its records replaced
+// the terms in u[]), then the running maximum and the bin index.
 __device__ __forceinline__ void
-k_sorted_uniforms_body(EngineRef eng, const ResampleCtl *ctl,
-                       const double *tile_excl, double *u, int32_t *L, int bid,
-                       SmemSortedUniforms &sm, long long spec_N = 0)
+k_sorted_uniforms_body(const ResampleCtl *ctl, const ExactScan exu,
+                       double *u, int32_t *L, int bid, SmemSortedUniforms &sm,
+                       long long spec_N = 0)
 {
     const SortedRun q = sorted_run(ctl, spec_N);
     if (!q.run)
         return;
-    double *sh = sm.sh;
     double *shm = sm.shm;
     const long long NN = q.NN;
     const long long base = (long long)bid * kTile;
     if (base >= NN)
         return;
-    const long long last = min(base + (long long)kTile, NN) - 1;
-    double t[kItems];
     const long long n0 = base + (long long)threadIdx.x * kItems;
+    // the thread's records (vector loads; u is padded past NN)
+    double rv[kItems];
 #pragma unroll
     for (int j = 0; j < kItems; ++j)
-        t[j] = n0 + j < NN ? u[n0 + j] : 0.0; // pass 1 stored the terms
-    double run = 0.0;
+        rv[j] = 0.0;
+    if (n0 < NN) {
+        const double2 *r2 = reinterpret_cast<const double2 *>(u + n0);
+#pragma unroll
+        for (int j = 0; j < kItems / 2; ++j) {
+            const double2 v = r2[j];
+            rv[2 * j] = n0 + 2 * j < NN ? v.x : 0.0;
+            rv[2 * j + 1] = n0 + 2 * j + 1 < NN ? v.y : 0.0;
+        }
+    }
+    const int nsp_tile = exu.tiles[bid].nspec;
+    if (nsp_tile <= kExactCap && (int)threadIdx.x < nsp_tile)
+        sm.sv[threadIdx.x] = exu.s_spec[(size_t)bid * kExactCap + threadIdx.x];
+    int nsp = 0;
 #pragma unroll
     for (int j = 0; j < kItems; ++j)
-        run += t[j];
-    double total;
-    double pre = block_excl_scan(run, sh, total);
-    const double a = tile_excl[bid];
-    const double b = tile_excl[bid + 1];
-    // carry: the previous tile ends exactly at lmax = a
-    const double umax = bid > 0 ? __dadd_rn(1.0, -fm::fm_exp(a)) : -INFINITY;
+        nsp += rv[j] < 0.0;
+    int nspec;
+    const int rank0 = block_excl_scan(nsp, sm.shi, nspec); // ends with a barrier
+    const double a = exu.start[bid]; // -lmax before the tile
+    double S[kItems];
+    exact_values(rv, rank0, a, sm.sv, nsp_tile > kExactCap, S);
+    // carry: the previous tile ends exactly at lmax = -a
+    const double umax = bid > 0 ? __dadd_rn(1.0, -fm::fm_exp(-a)) : -INFINITY;
     double uv[kItems];
     double tmax = -INFINITY;
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-        pre += t[j];
-        double lmax = fmax(__dadd_rn(a, pre), b); // lmax is non-increasing
-        if (n0 + j == last)
-            lmax = b;
-        uv[j] = __dadd_rn(1.0, -fm::fm_exp(lmax));
+        uv[j] = __dadd_rn(1.0, -fm::fm_exp(-S[j]));
         tmax = fmax(tmax, uv[j]);
     }
     // block exclusive max-scan (max is exact, so any order gives the same
@@ -770,11 +839,11 @@ k_sorted_uniforms_body(EngineRef eng, const ResampleCtl *ctl,
 }
 
 static __global__ void __launch_bounds__(VSMC_SCAN_BOUNDS)
-k_sorted_uniforms(EngineRef eng, const ResampleCtl *ctl,
-                  const double *tile_excl, double *u, int32_t *L)
+k_sorted_uniforms(const ResampleCtl *ctl, ExactScan exu, double *u,
+                  int32_t *L)
 {
     __shared__ SmemSortedUniforms sm;
-    k_sorted_uniforms_body(eng, ctl, tile_excl, u, L, blockIdx.x, sm);
+    k_sorted_uniforms_body(ctl, exu, u, L, blockIdx.x, sm);
 }
 
 // The speculative Multinomial sequence (N uniforms at the engine's current
@@ -796,11 +865,11 @@ k_spec_spine(const double *tile_sum, double *tile_excl,
 }
 
 static __global__ void __launch_bounds__(VSMC_SCAN_BOUNDS)
-k_spec_uniforms(EngineRef eng, const ResampleCtl *ctl, long long N,
-                const double *tile_excl, double *u, int32_t *L)
+k_spec_uniforms(const ResampleCtl *ctl, long long N, ExactScan exu, double *u,
+                int32_t *L)
 {
     __shared__ SmemSortedUniforms sm;
-    k_sorted_uniforms_body(eng, ctl, tile_excl, u, L, blockIdx.x, sm, N);
+    k_sorted_uniforms_body(ctl, exu, u, L, blockIdx.x, sm, N);
 }
 
 // The held sequence is now the one for the current position (launched
@@ -992,7 +1061,10 @@ k_exact_tiles_body(W wsrc, long long N, const ResampleCtl *ctl,
                    const double *tile_excl, ExactScan ex, int tile,
                    SmemExactTiles<Residual> &sm)
 {
-    if (!ctl->active)
+    if (!wsrc.active(ctl))
+        return;
+    N = wsrc.length(ctl, N);
+    if ((long long)tile * kTile >= N)
         return;
     // residual schemes without residual children scan nothing (the
     // inversion still takes the integer parts)
@@ -1125,9 +1197,11 @@ __device__ __forceinline__ void
 k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
                    ExactScan ex, SmemExactSpine &sm)
 {
-    if (!ctl->active || (Residual && ctl->NN <= 0))
+    if (!wsrc.active(ctl) || (Residual && ctl->NN <= 0))
         return;
     wsrc.prepare();
+    N = wsrc.length(ctl, N);
+    nt = min(nt, resample_ntiles(N));
     const int bd = (int)blockDim.x;
     const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5, nw = bd >> 5;
     const int perw = (nt + nw - 1) / nw;
@@ -1874,12 +1948,10 @@ struct ResampleWorkspace {
     double *u;             // N
     int32_t *sinc;         // N (tile-local surplus counts)
     ExactScan ex;          // the exact cumulative weight (exact_scan.cuh)
+    ExactScan exu;         // the exact lmax of the sorted U01 sequence
+                           // (its records live in u)
 };
 
-constexpr int resample_ntiles(long long N)
-{
-    return (int)((N + kTile - 1) / kTile);
-}
 
 constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
@@ -1896,13 +1968,23 @@ constexpr size_t exact_scan_bytes(long long N)
            2 * align256(nt * 4);
 }
 
+// The per-tile arrays of an exact scan whose records live elsewhere.
+constexpr size_t exact_scan_tile_bytes(long long N)
+{
+    const size_t nt = (size_t)resample_ntiles(N) + 1;
+    return align256(nt * sizeof(ExactTile)) +
+           align256(nt * kExactCap * sizeof(ExactSpecial)) +
+           align256(nt * kExactCap * 8) + 3 * align256(nt * 8) +
+           2 * align256(nt * 4);
+}
+
 constexpr size_t resample_workspace_bytes(long long N)
 {
     const size_t nt = (size_t)resample_ntiles(N) + 1;
     return align256(sizeof(ResampleCtl)) + 6 * align256(nt * 8) +
            5 * align256(nt * 4) + align256(((size_t)N / 8 + 2) * 4) +
            align256((size_t)N * 8) + align256((size_t)N * 4) +
-           exact_scan_bytes(N);
+           exact_scan_bytes(N) + exact_scan_tile_bytes(N);
 }
 
 inline ResampleWorkspace carve_workspace(void *base, long long N)
@@ -1959,6 +2041,24 @@ inline ResampleWorkspace carve_workspace(void *base, long long N)
     w.ex.dirty = reinterpret_cast<int32_t *>(p);
     p += align256(nt * 4);
     w.ex.eaft = reinterpret_cast<int32_t *>(p);
+    p += align256(nt * 4);
+    w.exu.tiles = reinterpret_cast<ExactTile *>(p);
+    p += align256(nt * sizeof(ExactTile));
+    w.exu.spec = reinterpret_cast<ExactSpecial *>(p);
+    p += align256(nt * kExactCap * sizeof(ExactSpecial));
+    w.exu.s_spec = reinterpret_cast<double *>(p);
+    p += align256(nt * kExactCap * 8);
+    w.exu.start = reinterpret_cast<double *>(p);
+    p += align256(nt * 8);
+    w.exu.s_out = reinterpret_cast<double *>(p);
+    p += align256(nt * 8);
+    w.exu.pk = reinterpret_cast<unsigned long long *>(p);
+    p += align256(nt * 8);
+    w.exu.dirty = reinterpret_cast<int32_t *>(p);
+    p += align256(nt * 4);
+    w.exu.eaft = reinterpret_cast<int32_t *>(p);
+    w.exu.rec = w.u;
+    w.exu.kint = nullptr;
     return w;
 }
 
@@ -1984,7 +2084,7 @@ inline int resample_launches(int scheme, bool parity, bool exact_norm = false)
     else if (strat)
         n += 1;
     else if (!sys)
-        n += 3;
+        n += 5; // sorted sequence: terms, spine, exact scan, uniforms
     return n;
 }
 
@@ -2079,8 +2179,13 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
                                                         ws.u_tile_sum, ws.u);
         k_sorted_spine<<<1, kSpineThreads, 0, s>>>(ws.u_tile_sum,
                                                    ws.u_tile_excl, ws.ctl);
-        k_sorted_uniforms<<<ntu_dev, kThreads, 0, s>>>(eng, ws.ctl,
-                                                       ws.u_tile_excl, ws.u,
+        // lmax exactly: the exact scan of the negated terms
+        const TermsNeg tn{ws.u, 0};
+        k_exact_tiles<TermsNeg, false><<<ntu_dev, kThreads, 0, s>>>(
+            tn, Nu, ws.ctl, ws.u_tile_excl, ws.exu);
+        k_exact_spine<TermsNeg, false><<<1, kSpineThreads, 0, s>>>(
+            tn, Nu, ws.ctl, ntu_dev, ws.exu);
+        k_sorted_uniforms<<<ntu_dev, kThreads, 0, s>>>(ws.ctl, ws.exu, ws.u,
                                                        ws.bins);
     }
     const long long *kex = residual ? ws.tile_kexcl : nullptr;
@@ -2213,7 +2318,7 @@ inline void launch_expand(const int32_t *rep, long long M, long long N,
 }
 
 // The speculative Multinomial sequence for the next resampling (see
-// sorted_run); 4 launches on `s`.
+// sorted_run); 6 launches on `s`.
 inline void launch_spec_sorted(long long N, const EngineRef &eng,
                                ResampleWorkspace &ws, cudaStream_t s)
 {
@@ -2222,8 +2327,13 @@ inline void launch_spec_sorted(long long N, const EngineRef &eng,
                                              ws.u);
     k_spec_spine<<<1, kSpineThreads, 0, s>>>(ws.u_tile_sum, ws.u_tile_excl,
                                              ws.ctl, N);
-    k_spec_uniforms<<<nt, kThreads, 0, s>>>(eng, ws.ctl, N, ws.u_tile_excl,
-                                            ws.u, ws.bins);
+    const TermsNeg tn{ws.u, N};
+    k_exact_tiles<TermsNeg, false><<<nt, kThreads, 0, s>>>(
+        tn, N, ws.ctl, ws.u_tile_excl, ws.exu);
+    k_exact_spine<TermsNeg, false><<<1, kSpineThreads, 0, s>>>(
+        tn, N, ws.ctl, nt, ws.exu);
+    k_spec_uniforms<<<nt, kThreads, 0, s>>>(ws.ctl, N, ws.exu, ws.u,
+                                            ws.bins);
     k_spec_commit<<<1, 1, 0, s>>>(ws.ctl);
 }
 
