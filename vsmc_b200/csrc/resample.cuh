@@ -127,7 +127,14 @@ constexpr int resample_ntiles(long long N)
 // Normalised weights given in memory (generic C ABI).
 struct WeightsGiven {
     static constexpr bool kExactNorm = false;
+    typedef double stage_t; // the per-element value a kernel stages
     const double *w;
+    __device__ __forceinline__ const double *stage_src() const { return w; }
+    __device__ __forceinline__ double from_stage(double x) const { return x; }
+    __device__ __forceinline__ double unnorm_stage(double x) const
+    {
+        return x;
+    }
     __device__ __forceinline__ void prepare() {}
     __device__ __forceinline__ double operator()(long long i) const
     {
@@ -162,6 +169,7 @@ struct WeightsGiven {
 template <typename Real>
 struct WeightsFromLog {
     static constexpr bool kExactNorm = sizeof(Real) == sizeof(double);
+    typedef Real stage_t; // lw, or (FP64, raw set) the kept exp(lw - M)
     const Real *lw;
     const double *stats;       // [0] = M (max log-weight), [1] = S1
     const double *coeff_exact = nullptr; // the sequential sum's reciprocal
@@ -175,6 +183,12 @@ struct WeightsFromLog {
     }
     __device__ __forceinline__ double operator()(long long i) const;
     __device__ __forceinline__ double unnorm(long long i) const;
+    __device__ __forceinline__ const Real *stage_src() const;
+    __device__ __forceinline__ double unnorm_stage(Real x) const;
+    __device__ __forceinline__ double from_stage(Real x) const
+    {
+        return __dmul_rn(unnorm_stage(x), coeff);
+    }
     // the approximate spine (tile statistics scaled by coeff_apx) relative
     // to these weights' scale, and to the unnormalised weights'
     __device__ __forceinline__ double spine_ratio() const
@@ -211,6 +225,34 @@ WeightsFromLog<double>::operator()(long long i) const
 }
 
 template <>
+__device__ __forceinline__ const double *
+WeightsFromLog<double>::stage_src() const
+{
+    return raw != nullptr ? raw : lw;
+}
+
+template <>
+__device__ __forceinline__ double
+WeightsFromLog<double>::unnorm_stage(double x) const
+{
+    return raw != nullptr ? x : fm::fm_exp(__dadd_rn(x, -M));
+}
+
+template <>
+__device__ __forceinline__ const float *
+WeightsFromLog<float>::stage_src() const
+{
+    return lw;
+}
+
+template <>
+__device__ __forceinline__ double
+WeightsFromLog<float>::unnorm_stage(float x) const
+{
+    return static_cast<double>(expf(x - static_cast<float>(M)));
+}
+
+template <>
 __device__ __forceinline__ double
 WeightsFromLog<float>::unnorm(long long i) const
 {
@@ -223,8 +265,15 @@ WeightsFromLog<float>::unnorm(long long i) const
 // sequence of spec_N uniforms (sorted_run).
 struct TermsNeg {
     static constexpr bool kExactNorm = false;
+    typedef double stage_t;
     const double *u;
     long long spec_N;
+    __device__ __forceinline__ const double *stage_src() const { return u; }
+    __device__ __forceinline__ double from_stage(double x) const { return -x; }
+    __device__ __forceinline__ double unnorm_stage(double x) const
+    {
+        return -x;
+    }
     __device__ __forceinline__ void prepare() {}
     __device__ __forceinline__ double operator()(long long i) const
     {
@@ -1041,20 +1090,126 @@ __device__ __forceinline__ double scan_weight(const W &wsrc, long long i,
     return w;
 }
 
-template <bool Residual>
-struct SmemExactTiles {
-    double sw[kTile];                // weights, then the records
-    int32_t sk[Residual ? kTile : 1]; // floor(N w)
+// A tile's values in shared memory are padded by one slot per 8, so that a
+// thread reading its kItems consecutive values meets no bank conflict.
+constexpr int kTilePad = kTile + kTile / 8;
+__device__ __forceinline__ int pad8(int l) { return l + (l >> 3); }
+
+struct SmemExactCore {
     double shd[kThreads / 32];
     SmemExactThread et;
 };
 
-// Phase A of the exact cumulative weight (exact_scan.cuh) for one tile.
+template <bool Residual>
+struct SmemExactTiles {
+    double sw[kTilePad];
+    int32_t sk[Residual ? kTilePad : 1]; // floor(N w)
+    SmemExactCore core;
+};
+
+// The weight scanned for a value staged from the source's array.
+template <typename W, bool Residual, bool Raw>
+__device__ __forceinline__ double
+scan_weight_staged(const W &wsrc, typename W::stage_t x, double Nd,
+                   double coeff_r, double &kint)
+{
+    double w, k = 0.0;
+    if (Raw && !Residual) {
+        w = wsrc.unnorm_stage(x);
+    } else {
+        w = wsrc.from_stage(x);
+        if (Residual)
+            w = __dmul_rn(residual_split(w, Nd, k), coeff_r);
+    }
+    kint = k;
+    return w;
+}
+
+// Eight values of a thread to global memory (vector stores when all are
+// below N).
+template <typename T>
+__device__ __forceinline__ void store8(T *dst, long long i0, long long N,
+                                       const T (&v)[kItems])
+{
+    if (i0 + kItems <= N) {
+        if (sizeof(T) == 8) {
+            double2 *d = reinterpret_cast<double2 *>(dst + i0);
+#pragma unroll
+            for (int j = 0; j < kItems / 2; ++j) {
+                double2 q;
+                q.x = *reinterpret_cast<const double *>(&v[2 * j]);
+                q.y = *reinterpret_cast<const double *>(&v[2 * j + 1]);
+                d[j] = q;
+            }
+        } else {
+            int4 *d = reinterpret_cast<int4 *>(dst + i0);
+#pragma unroll
+            for (int j = 0; j < kItems / 4; ++j) {
+                int4 q;
+                q.x = *reinterpret_cast<const int *>(&v[4 * j]);
+                q.y = *reinterpret_cast<const int *>(&v[4 * j + 1]);
+                q.z = *reinterpret_cast<const int *>(&v[4 * j + 2]);
+                q.w = *reinterpret_cast<const int *>(&v[4 * j + 3]);
+                d[j] = q;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < kItems; ++j)
+            if (i0 + j < N)
+                dst[i0 + j] = v[j];
+    }
+}
+
+// Phase A of the exact cumulative weight (exact_scan.cuh) for one tile,
+// given the thread's kItems weights w (and, residual, integer parts kk).
 // Raw: the weights' or the residuals' sequential sum only (for their
-// coefficient); otherwise also the element records (and, residual, the
-// integer parts floor(N w)) for the inversion.  The approximate spine
-// tile_excl is of the weights (or residuals) scaled by the spine's
-// coefficient: it is rescaled to the weights scanned here.
+// coefficient); the normalisation pass also keeps the unnormalised
+// weights in ex.rec.  Otherwise also the element records (and, residual,
+// the integer parts floor(N w)) for the inversion; a tile with more
+// specials than kept keeps its values for the spine, which writes S itself
+// there.  The approximate spine tile_excl is of the weights (or residuals)
+// scaled by the spine's coefficient: it is rescaled to the weights scanned
+// here.
+template <typename W, bool Residual, bool Raw>
+__device__ __forceinline__ void
+exact_tile_compute(const W &wsrc, long long N, const ResampleCtl *ctl,
+                   const double *tile_excl, const ExactScan &ex, int tile,
+                   double coeff_r, const double (&w)[kItems],
+                   const int32_t (&kk)[kItems], SmemExactCore &sm)
+{
+    const long long base = (long long)tile * kTile;
+    double run = 0.0;
+#pragma unroll
+    for (int j = 0; j < kItems; ++j)
+        run += w[j];
+    double total;
+    const double pre = block_excl_scan(run, sm.shd, total);
+    const long long i0 = base + (long long)threadIdx.x * kItems;
+    double a_apx;
+    if (Residual)
+        a_apx = Raw ? __ddiv_rn(tile_excl[tile], ctl->coeff_r_apx)
+                    : __dmul_rn(tile_excl[tile],
+                                __ddiv_rn(coeff_r, ctl->coeff_r_apx));
+    else
+        a_apx = Raw ? __dmul_rn(tile_excl[tile], wsrc.spine_unnorm())
+                    : __dmul_rn(tile_excl[tile], wsrc.spine_ratio());
+    ExactThread x;
+    exact_thread(i0, N, w, a_apx, pre, ExactMargin<W>::rel, x, sm.et);
+    double rec[kItems];
+    exact_tile_record(x, w, base, i0, N, tile, ex, rec);
+    if (i0 < N) {
+        if (Raw && !Residual && W::kExactNorm)
+            store8(ex.rec, i0, N, w);
+        if (!Raw && x.nspec <= kExactCap)
+            store8(ex.rec, i0, N, rec);
+        if (!Raw && Residual)
+            store8(ex.kint, i0, N, kk);
+    }
+}
+
+// Phase A for one tile, reading the source in global memory (the batched
+// kernels' tile loops).
 template <typename W, bool Residual, bool Raw = false>
 __device__ __forceinline__ void
 k_exact_tiles_body(W wsrc, long long N, const ResampleCtl *ctl,
@@ -1089,58 +1244,23 @@ k_exact_tiles_body(W wsrc, long long N, const ResampleCtl *ctl,
                 ex.kint[i] = (int32_t)k;
             continue;
         }
-        sm.sw[l] = w;
+        sm.sw[pad8(l)] = w;
         if (Residual && !Raw)
-            sm.sk[l] = (int32_t)k;
-        if (Raw && !Residual && W::kExactNorm && i < N)
-            ex.rec[i] = w; // the unnormalised weights, for the later passes
+            sm.sk[pad8(l)] = (int32_t)k;
     }
     if (none)
         return;
     __syncthreads();
     double w[kItems];
-    double run = 0.0;
+    int32_t kk[kItems];
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-        w[j] = sm.sw[threadIdx.x * kItems + j];
-        run += w[j];
+        const int l = pad8(threadIdx.x * kItems + j);
+        w[j] = sm.sw[l];
+        kk[j] = Residual && !Raw ? sm.sk[l] : 0;
     }
-    double total;
-    const double pre = block_excl_scan(run, sm.shd, total);
-    const long long i0 = base + (long long)threadIdx.x * kItems;
-    double a_apx;
-    if (Residual)
-        a_apx = Raw ? __ddiv_rn(tile_excl[tile], ctl->coeff_r_apx)
-                    : __dmul_rn(tile_excl[tile],
-                                __ddiv_rn(coeff_r, ctl->coeff_r_apx));
-    else
-        a_apx = Raw ? __dmul_rn(tile_excl[tile], wsrc.spine_unnorm())
-                    : __dmul_rn(tile_excl[tile], wsrc.spine_ratio());
-    ExactThread x;
-    exact_thread(i0, N, w, a_apx, pre, ExactMargin<W>::rel, x, sm.et);
-    double rec[kItems];
-    exact_tile_record(x, w, base, i0, N, tile, ex, rec);
-    if (!Raw) {
-        // the records (and integer parts) out with coalesced stores; a tile
-        // with more specials than kept keeps its unnormalised weights for
-        // the spine, which writes S itself there
-        const bool overflow = x.nspec > kExactCap;
-#pragma unroll
-        for (int j = 0; j < kItems; ++j)
-            sm.sw[threadIdx.x * kItems + j] = rec[j];
-        __syncthreads();
-#pragma unroll
-        for (int j = 0; j < kItems; ++j) {
-            const int l = j * kThreads + threadIdx.x;
-            const long long i = base + l;
-            if (i < N) {
-                if (!overflow)
-                    ex.rec[i] = sm.sw[l];
-                if (Residual)
-                    ex.kint[i] = sm.sk[l];
-            }
-        }
-    }
+    exact_tile_compute<W, Residual, Raw>(wsrc, N, ctl, tile_excl, ex, tile,
+                                         coeff_r, w, kk, sm.core);
 }
 
 // Four CTAs per SM (64 registers, a few spilled) hide the exact scan's
@@ -1150,14 +1270,123 @@ k_exact_tiles_body(W wsrc, long long N, const ResampleCtl *ctl,
 #define VSMC_EXACT_MIN_BLOCKS 4
 #endif
 
+template <int Bytes>
+__device__ __forceinline__ void cp_async_n(void *smem, const void *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    if (Bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa),
+                     "l"(gmem)
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa),
+                     "l"(gmem)
+                     : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_one()
+{
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
+
+// CTAs per SM of the staging k_exact_tiles: the prefetch hides the load
+// latency, so three CTAs (85 registers) do without four's spills.
+#ifndef VSMC_EXACT_STAGE_MIN_BLOCKS
+#define VSMC_EXACT_STAGE_MIN_BLOCKS 3
+#endif
+
+// The persistent grid of k_exact_tiles for nt tiles: the SMs times the
+// CTAs that fit on one, or fewer for small filters.
+inline int exact_grid(int nt)
+{
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0, v = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) ==
+                cudaSuccess &&
+            v > 0)
+            sms = v;
+        else
+            sms = 148;
+    }
+    const int g = sms * VSMC_EXACT_STAGE_MIN_BLOCKS;
+    return nt < 1 ? 1 : (nt < g ? nt : g);
+}
+
+struct SmemExactStage {
+    double stage[2][kTilePad]; // the source's values of two tiles
+    SmemExactCore core;
+};
+
+// Phase A over every tile: a persistent grid (the SMs times the CTAs that
+// fit on one) whose CTAs stage the next tile's source values with cp.async
+// while they classify the current one, so the loads' latency is hidden.
 template <typename W, bool Residual, bool Raw = false>
-__global__ void __launch_bounds__(kThreads, VSMC_EXACT_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, VSMC_EXACT_STAGE_MIN_BLOCKS)
 k_exact_tiles(W wsrc, long long N, const ResampleCtl *ctl,
               const double *tile_excl, ExactScan ex)
 {
-    __shared__ SmemExactTiles<Residual> sm;
-    k_exact_tiles_body<W, Residual, Raw>(wsrc, N, ctl, tile_excl, ex,
-                                         blockIdx.x, sm);
+    typedef typename W::stage_t S;
+    __shared__ SmemExactStage sm;
+    if (!wsrc.active(ctl))
+        return;
+    N = wsrc.length(ctl, N);
+    const bool none = Residual && ctl->NN <= 0;
+    if (none && Raw)
+        return;
+    wsrc.prepare();
+    const int nt = resample_ntiles(N);
+    const double Nd = (double)resample_children(ctl, N);
+    const double coeff_r = Residual && !Raw ? ctl->coeff_r : 1.0;
+    const S *src = wsrc.stage_src();
+    const auto issue = [&](int t, int b) {
+        S *dst = reinterpret_cast<S *>(sm.stage[b]);
+        const long long base = (long long)t * kTile;
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) {
+            const int l = j * kThreads + threadIdx.x;
+            if (base + l < N)
+                cp_async_n<sizeof(S)>(&dst[pad8(l)], &src[base + l]);
+        }
+        cp_async_commit();
+    };
+    int buf = 0;
+    if ((int)blockIdx.x < nt)
+        issue(blockIdx.x, 0);
+    for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+        const int next = tile + gridDim.x;
+        if (next < nt) {
+            issue(next, buf ^ 1);
+            cp_async_wait_one();
+        } else {
+            cp_async_wait_all();
+        }
+        __syncthreads();
+        const S *st = reinterpret_cast<const S *>(sm.stage[buf]);
+        const long long i0 =
+            (long long)tile * kTile + (long long)threadIdx.x * kItems;
+        double w[kItems];
+        int32_t kk[kItems];
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) {
+            double k = 0.0;
+            w[j] = i0 + j < N ? scan_weight_staged<W, Residual, Raw>(
+                                    wsrc, st[pad8(threadIdx.x * kItems + j)],
+                                    Nd, coeff_r, k)
+                              : 0.0;
+            kk[j] = (int32_t)k;
+        }
+        if (none) {
+            if (i0 < N)
+                store8(ex.kint, i0, N, kk);
+        } else {
+            exact_tile_compute<W, Residual, Raw>(wsrc, N, ctl, tile_excl, ex,
+                                                 tile, coeff_r, w, kk,
+                                                 sm.core);
+        }
+        __syncthreads(); // every read of stage[buf] before it is refilled
+        buf ^= 1;
+    }
 }
 
 constexpr int kExactDirtyStage = 256; // tiles with specials the spine stages
@@ -2128,7 +2357,7 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
                     ws.tile_sum, nullptr, ws.tile_excl, nullptr, nt, N, eng,
                     ws.ctl);
         }
-        k_exact_tiles<W, false, true><<<nt, kThreads, 0, s>>>(
+        k_exact_tiles<W, false, true><<<exact_grid(nt), kThreads, 0, s>>>(
             wsrc, N, ws.ctl, ws.tile_excl, ws.ex);
         k_exact_spine<W, false, true><<<1, kSpineThreads, 0, s>>>(
             wsrc, N, ws.ctl, nt, ws.ex);
@@ -2181,7 +2410,7 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
                                                    ws.u_tile_excl, ws.ctl);
         // lmax exactly: the exact scan of the negated terms
         const TermsNeg tn{ws.u, 0};
-        k_exact_tiles<TermsNeg, false><<<ntu_dev, kThreads, 0, s>>>(
+        k_exact_tiles<TermsNeg, false><<<exact_grid(ntu_dev), kThreads, 0, s>>>(
             tn, Nu, ws.ctl, ws.u_tile_excl, ws.exu);
         k_exact_spine<TermsNeg, false><<<1, kSpineThreads, 0, s>>>(
             tn, Nu, ws.ctl, ntu_dev, ws.exu);
@@ -2193,16 +2422,16 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
     // residual schemes first the sum of the residuals, whose reciprocal
     // scales them)
     if (residual) {
-        k_exact_tiles<W, true, true><<<nt, kThreads, 0, s>>>(
+        k_exact_tiles<W, true, true><<<exact_grid(nt), kThreads, 0, s>>>(
             wx, N, ws.ctl, ws.tile_excl, ws.ex);
         k_exact_spine<W, true, true><<<1, kSpineThreads, 0, s>>>(
             wx, N, ws.ctl, nt, ws.ex);
-        k_exact_tiles<W, true><<<nt, kThreads, 0, s>>>(wx, N, ws.ctl,
+        k_exact_tiles<W, true><<<exact_grid(nt), kThreads, 0, s>>>(wx, N, ws.ctl,
                                                        ws.tile_excl, ws.ex);
         k_exact_spine<W, true><<<1, kSpineThreads, 0, s>>>(wx, N, ws.ctl,
                                                            nt, ws.ex);
     } else {
-        k_exact_tiles<W, false><<<nt, kThreads, 0, s>>>(wx, N, ws.ctl,
+        k_exact_tiles<W, false><<<exact_grid(nt), kThreads, 0, s>>>(wx, N, ws.ctl,
                                                         ws.tile_excl, ws.ex);
         k_exact_spine<W, false><<<1, kSpineThreads, 0, s>>>(wx, N, ws.ctl,
                                                             nt, ws.ex);
@@ -2328,7 +2557,7 @@ inline void launch_spec_sorted(long long N, const EngineRef &eng,
     k_spec_spine<<<1, kSpineThreads, 0, s>>>(ws.u_tile_sum, ws.u_tile_excl,
                                              ws.ctl, N);
     const TermsNeg tn{ws.u, N};
-    k_exact_tiles<TermsNeg, false><<<nt, kThreads, 0, s>>>(
+    k_exact_tiles<TermsNeg, false><<<exact_grid(nt), kThreads, 0, s>>>(
         tn, N, ws.ctl, ws.u_tile_excl, ws.exu);
     k_exact_spine<TermsNeg, false><<<1, kSpineThreads, 0, s>>>(
         tn, N, ws.ctl, nt, ws.exu);
