@@ -418,7 +418,12 @@ int vsmc_cuda_cv_create(const vsmc_cuda_cv_config *cfg, void *stream,
     f->move_grid = (int)f->ntiles;
     e = cudaMemsetAsync(f->mem, 0, f->bytes, f->stream);
     if (e == cudaSuccess && cfg->scheme == VSMC_CUDA_MULTINOMIAL) {
-        e = cudaStreamCreateWithFlags(&f->side, cudaStreamNonBlocking);
+        // the lowest priority: the sequence fills SMs the step's own
+        // kernels leave idle (the one-CTA finalize and spines) instead of
+        // competing with the move
+        int lo = 0, hi = 0;
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        e = cudaStreamCreateWithPriority(&f->side, cudaStreamNonBlocking, lo);
         if (e == cudaSuccess)
             e = cudaEventCreateWithFlags(&f->ev_pos, cudaEventDisableTiming);
         if (e == cudaSuccess)
