@@ -198,3 +198,50 @@ def test_filter_near_maximum_size(capi, form):
         assert np.all(np.isfinite(h[k])), k
         assert np.array_equal(h[k], runs[1][k]), k
     assert np.isfinite(h["logz"]) and h["logz"] == runs[1]["logz"]
+
+
+@pytest.mark.parametrize("sch", range(6))
+@pytest.mark.parametrize("N", [5000, (1 << 16) + 37])
+def test_mixed_form_plain_scan_resampling(capi, N, sch):
+    """The mixed form's float weights are not the reference's bit for bit,
+    so its cumulative weight is a plain FP64 scan (per-tile prefixes on an
+    exact fixed-point spine of the tile totals) rather than the reference's
+    sequential sum.  On the FP64 run's trajectory (compare mode: the mixed
+    filter follows the FP64 copy_from while it records its own resampling
+    of its own weights) every resampling is a valid cfrp_trans ancestry --
+    indices in range, each parent with children keeps its own slot -- and
+    its replication counts differ from the FP64 form's in a small fraction
+    of particles (the float weights' rounding moves a uniform across a
+    cumulative weight only where the two lie that close)."""
+    import torch
+
+    T = 8
+    ox, oy = O.cv_simulate(T, obs_seed=3)
+    rec64 = torch.full((T, N), -1, dtype=torch.int32, device="cuda")
+    with capi.CVFilter(N, T, scheme=sch, threshold=1.1) as f:
+        f.set_ancestry(record_ptr=rec64.data_ptr())
+        f.set_observations_host(ox, oy)
+        f.initialize()
+        f.iterate(T - 1)
+        h64 = f.history()
+    assert np.all(h64["resampled"] == 1)
+    flags = torch.from_numpy(h64["resampled"].astype(np.int32)).cuda()
+    rec32 = torch.full((T, N), -1, dtype=torch.int32, device="cuda")
+    with capi.CVFilter(N, T, scheme=sch, form=capi.MIXED, threshold=1.1) as g:
+        g.set_ancestry(record_ptr=rec32.data_ptr(), replay_ptr=rec64.data_ptr(),
+                       replay_flags_ptr=flags.data_ptr())
+        g.set_observations_host(ox, oy)
+        g.initialize()
+        g.iterate(T - 1)
+        g.synchronize()
+    c64, c32 = rec64.cpu().numpy(), rec32.cpu().numpy()
+    diffs = []
+    for t in range(T):
+        cf = c32[t]
+        assert cf.min() >= 0 and cf.max() < N, t
+        rep = np.bincount(cf, minlength=N)
+        parents = np.nonzero(rep)[0]
+        assert np.array_equal(cf[parents], parents), t
+        diffs.append(int(np.abs(rep - np.bincount(c64[t], minlength=N)).sum()))
+    print(f"mixed plain scan N={N} scheme {sch}: |rep32 - rep64|_1 per step {diffs}")
+    assert max(diffs) <= 0.02 * N

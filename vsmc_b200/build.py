@@ -19,8 +19,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "lib", "libvsmc_cuda.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
          "--expt-relaxed-constexpr"]
+OBJ = os.path.join(HERE, "lib", "obj")
 
 
 def sources():
@@ -29,6 +30,7 @@ def sources():
 
 def _inputs():
     return (sources() + glob.glob(os.path.join(CSRC, "*.cuh"))
+            + glob.glob(os.path.join(ROOT, "include", "vsmc_b200", "*.cuh"))
             + [os.path.join(ROOT, "include", "vsmc_cuda.h")])
 
 
@@ -40,11 +42,24 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every translation unit to an object (in parallel, one nvcc
+    per source) and link the shared library."""
     if not force and up_to_date():
         return LIB
-    os.makedirs(os.path.dirname(LIB), exist_ok=True)
+    os.makedirs(OBJ, exist_ok=True)
+    objs, procs = [], []
+    for src in sources():
+        obj = os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
+        cmd = [NVCC, *ARCH, *FLAGS, "-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd))
+        objs.append(obj)
+        procs.append((subprocess.Popen(cmd), cmd))
+    failed = [cmd for p, cmd in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     tmp = LIB + ".tmp"
-    cmd = [NVCC, *ARCH, *FLAGS, "-o", tmp, *sources()]
+    cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

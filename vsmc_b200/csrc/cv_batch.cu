@@ -508,7 +508,8 @@ kb_block_run(BatchSlot *slots, const BlockItem *items, int n, int *queue,
                     __syncthreads();
                 }
             }
-            if constexpr (Residual) { // the residuals' exact sum
+            if constexpr (Residual && !WeightsFromLog<Real>::kApprox) {
+                // the residuals' exact sum
                 for (int tile = 0; tile < nt; ++tile) {
                     k_exact_tiles_body<WeightsFromLog<Real>, true, true>(
                         w, b.N, b.rws.ctl, b.rws.tile_excl, b.rws.ex, tile,
@@ -1032,12 +1033,14 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
         launches += 5;
     }
     if (residual) {
-        kb_exact_tiles<Real, true, true><<<nt, kThreads, 0, s>>>(sl, map);
-        kb_exact_spine<Real, true, true><<<n, kSpineThreads, 0, s>>>(sl,
-                                                                    work);
+        if (!WeightsFromLog<Real>::kApprox) { // the residuals' exact sum
+            kb_exact_tiles<Real, true, true><<<nt, kThreads, 0, s>>>(sl, map);
+            kb_exact_spine<Real, true, true><<<n, kSpineThreads, 0, s>>>(
+                sl, work);
+            launches += 2;
+        }
         kb_exact_tiles<Real, true><<<nt, kThreads, 0, s>>>(sl, map);
         kb_exact_spine<Real, true><<<n, kSpineThreads, 0, s>>>(sl, work);
-        launches += 2;
     } else {
         kb_exact_tiles<Real, false><<<nt, kThreads, 0, s>>>(sl, map);
         kb_exact_spine<Real, false><<<n, kSpineThreads, 0, s>>>(sl, work);

@@ -221,7 +221,8 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
                                  /*spine_done=*/true, nullptr,
                                  f->rec_cf + (size_t)f->iter * c.N, s);
             f->launches += resample_launches(c.scheme, false,
-                                           WeightsFromLog<Real>::kExactNorm);
+                                           WeightsFromLog<Real>::kExactNorm,
+                                           WeightsFromLog<Real>::kApprox);
         }
         // replay: the recorded ancestry of this step (used only if the
         // recorded decision was to resample)
@@ -244,7 +245,8 @@ void launch_step(vsmc_cuda_cv_filter *f, bool init)
     if (ev)
         cudaEventRecord(ev[2], s);
     f->launches += 2 + resample_launches(c.scheme, false,
-                                           WeightsFromLog<Real>::kExactNorm);
+                                           WeightsFromLog<Real>::kExactNorm,
+                                           WeightsFromLog<Real>::kApprox);
     ++f->iter;
 }
 

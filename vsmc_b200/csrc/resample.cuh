@@ -127,6 +127,7 @@ constexpr int resample_ntiles(long long N)
 // Normalised weights given in memory (generic C ABI).
 struct WeightsGiven {
     static constexpr bool kExactNorm = false;
+    static constexpr bool kApprox = false;
     typedef double stage_t; // the per-element value a kernel stages
     const double *w;
     __device__ __forceinline__ const double *stage_src() const { return w; }
@@ -169,6 +170,11 @@ struct WeightsGiven {
 template <typename Real>
 struct WeightsFromLog {
     static constexpr bool kExactNorm = sizeof(Real) == sizeof(double);
+    // The mixed form's weights are not the reference's bit for bit (float
+    // log-weights), so the reference's sequential cumulative sum has nothing
+    // to reproduce there: its cumulative weight is a plain FP64 scan
+    // (approx_tile_compute / approx_spine).
+    static constexpr bool kApprox = sizeof(Real) == sizeof(float);
     typedef Real stage_t; // lw, or (FP64, raw set) the kept exp(lw - M)
     const Real *lw;
     const double *stats;       // [0] = M (max log-weight), [1] = S1
@@ -265,6 +271,7 @@ WeightsFromLog<float>::unnorm(long long i) const
 // sequence of spec_N uniforms (sorted_run).
 struct TermsNeg {
     static constexpr bool kExactNorm = false;
+    static constexpr bool kApprox = false;
     typedef double stage_t;
     const double *u;
     long long spec_N;
@@ -326,15 +333,10 @@ WeightsFromLog<float>::operator()(long long i) const
 
 // Relative error margin of the approximate cumulative weights the exact
 // scan classifies with (its spine comes from the weights' tile sums): FP64
-// weights carry a few ulps; weights of a float form differ from the move's
-// per-tile sums by the float rounding of lw - max (about 1e-6 relative).
+// weights carry a few ulps.
 template <typename W>
 struct ExactMargin {
     static constexpr double rel = 0x1p-44;
-};
-template <>
-struct ExactMargin<WeightsFromLog<float> > {
-    static constexpr double rel = 0x1p-19;
 };
 
 // Residual split of a weight: r = modf(N w, &k) (residual.hpp:61-62).
@@ -1161,6 +1163,72 @@ __device__ __forceinline__ void store8(T *dst, long long i0, long long N,
     }
 }
 
+// The mixed form's cumulative weight: a plain FP64 scan.  Each element's
+// record is its inclusive prefix within the tile (a block scan of the
+// thread's sequential run); the tile's total goes to the spine as an
+// unsigned 2^-60 fixed-point integer, so that the tile starts are an exact
+// integer scan (non-decreasing whatever the association, hence the same in
+// every launch shape) rounded once to double.  The weights are normalised
+// (total about 1); totals are clamped to [0, 8] and NaN counts as 0.  The
+// inversion gives each tile's last particle the uniforms up to the next
+// tile's start, so the records' rounding cannot lose or repeat a child.
+constexpr double kApproxScale = 0x1p60;
+
+__device__ __forceinline__ unsigned long long approx_fixed(double x)
+{
+    if (!(x > 0.0))
+        return 0ull;
+    return __double2ull_rn(__dmul_rn(fmin(x, 8.0), kApproxScale));
+}
+
+template <bool Residual>
+__device__ __forceinline__ void
+approx_tile_record(const double (&w)[kItems], const int32_t (&kk)[kItems],
+                   double pre, double total, long long N, long long i0,
+                   int tile, const ExactScan &ex)
+{
+    double rec[kItems];
+    double s = pre;
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        s += w[j];
+        rec[j] = s;
+    }
+    if (i0 < N) {
+        store8(ex.rec, i0, N, rec);
+        if (Residual)
+            store8(ex.kint, i0, N, kk);
+    }
+    if (threadIdx.x == 0) {
+        ExactTile et;
+        et.k_total = 0;
+        et.nspec = 0;
+        et.e_last = kNoBinade;
+        ex.tiles[tile] = et;
+        ex.pk[tile] = approx_fixed(total);
+    }
+}
+
+// The tile starts of the plain scan (one CTA): the exclusive integer scan
+// of the tiles' fixed-point totals, each rounded once to double.
+__device__ __forceinline__ void approx_spine(const ExactScan &ex, int nt,
+                                             unsigned long long *sh)
+{
+    const int per = (nt + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int b = (int)threadIdx.x * per, e = min(b + per, nt);
+    unsigned long long run = 0;
+    for (int t = b; t < e; ++t)
+        run += ex.pk[t];
+    unsigned long long total;
+    unsigned long long off = block_excl_scan(run, sh, total);
+    for (int t = b; t < e; ++t) {
+        ex.start[t] = __dmul_rn(__ull2double_rn(off), 1.0 / kApproxScale);
+        off += ex.pk[t];
+    }
+    if (threadIdx.x == blockDim.x - 1)
+        ex.start[nt] = __dmul_rn(__ull2double_rn(total), 1.0 / kApproxScale);
+}
+
 // Phase A of the exact cumulative weight (exact_scan.cuh) for one tile,
 // given the thread's kItems weights w (and, residual, integer parts kk).
 // Raw: the weights' or the residuals' sequential sum only (for their
@@ -1186,6 +1254,11 @@ exact_tile_compute(const W &wsrc, long long N, const ResampleCtl *ctl,
     double total;
     const double pre = block_excl_scan(run, sm.shd, total);
     const long long i0 = base + (long long)threadIdx.x * kItems;
+    if (W::kApprox) {
+        if (!Raw)
+            approx_tile_record<Residual>(w, kk, pre, total, N, i0, tile, ex);
+        return;
+    }
     double a_apx;
     if (Residual)
         a_apx = Raw ? __ddiv_rn(tile_excl[tile], ctl->coeff_r_apx)
@@ -1431,6 +1504,13 @@ k_exact_spine_body(W wsrc, long long N, ResampleCtl *ctl, int nt,
     wsrc.prepare();
     N = wsrc.length(ctl, N);
     nt = min(nt, resample_ntiles(N));
+    if (W::kApprox) {
+        // the plain scan's tile starts (the coefficients stay the tile
+        // sums' approximate ones)
+        if (!Raw)
+            approx_spine(ex, nt, sm.wk);
+        return;
+    }
     const int bd = (int)blockDim.x;
     const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5, nw = bd >> 5;
     const int perw = (nt + nw - 1) / nw;
@@ -1771,6 +1851,7 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     int cnt[kItems];
     int pos = -1;
     long long gpos = -1;
+    const int tile_last = (int)min(base + (long long)kTile, N) - 1;
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
         const int i = i0 + j;
@@ -1778,6 +1859,9 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
         int c;
         if (i >= iN - 1) {
             c = iNN; // the last particle takes every remaining uniform
+        } else if (W::kApprox && i == tile_last) {
+            // the plain scan: the tile closes at the next tile's start
+            c = ihi;
         } else if (Sys) {
             c = (int)sys_count(C, u0, delta, NN);
         } else if (staged) {
@@ -1832,7 +1916,6 @@ k_invert_body(W wsrc, long long N, ResampleCtl *ctl, const double *tile_excl,
     const int kex = Residual ? block_excl_scan(ksum, shi, ktot) : 0;
     if (threadIdx.x == 0)
         tile_zeros[tile] = ztot;
-    const int tile_last = (int)min(base + (long long)kTile, N) - 1;
     int kprefix = Residual ? (int)tile_kexcl[tile] + kex : 0;
     int32_t cf[kItems], sc[kItems], rp[kItems];
 #pragma unroll
@@ -2292,8 +2375,10 @@ inline ResampleWorkspace carve_workspace(void *base, long long N)
 }
 
 // Kernels launch_resample_core issues (for the launch counters); the
-// filters' FP64 weights add the normalisation pass (exact_norm).
-inline int resample_launches(int scheme, bool parity, bool exact_norm = false)
+// filters' FP64 weights add the normalisation pass (exact_norm), the mixed
+// form's plain scan drops the residuals' exact sum (approx).
+inline int resample_launches(int scheme, bool parity, bool exact_norm = false,
+                             bool approx = false)
 {
     const bool residual = scheme == VSMC_CUDA_RESIDUAL ||
                           scheme == VSMC_CUDA_RESIDUAL_STRATIFIED ||
@@ -2305,7 +2390,7 @@ inline int resample_launches(int scheme, bool parity, bool exact_norm = false)
     int n = 5; // exact tiles and spine, invert, zero spine (and engine
                // position), cfrp fill
     if (residual)
-        n += 4; // tile sums, spine, the residuals' exact sum
+        n += approx ? 2 : 4; // tile sums, spine, the residuals' exact sum
     if (exact_norm)
         n += 2;
     if (parity)
@@ -2422,10 +2507,12 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
     // residual schemes first the sum of the residuals, whose reciprocal
     // scales them)
     if (residual) {
-        k_exact_tiles<W, true, true><<<exact_grid(nt), kThreads, 0, s>>>(
-            wx, N, ws.ctl, ws.tile_excl, ws.ex);
-        k_exact_spine<W, true, true><<<1, kSpineThreads, 0, s>>>(
-            wx, N, ws.ctl, nt, ws.ex);
+        if (!W::kApprox) {
+            k_exact_tiles<W, true, true><<<exact_grid(nt), kThreads, 0, s>>>(
+                wx, N, ws.ctl, ws.tile_excl, ws.ex);
+            k_exact_spine<W, true, true><<<1, kSpineThreads, 0, s>>>(
+                wx, N, ws.ctl, nt, ws.ex);
+        }
         k_exact_tiles<W, true><<<exact_grid(nt), kThreads, 0, s>>>(wx, N, ws.ctl,
                                                        ws.tile_excl, ws.ex);
         k_exact_spine<W, true><<<1, kSpineThreads, 0, s>>>(wx, N, ws.ctl,
