@@ -1003,21 +1003,25 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
     // while every slot has at most 256 tiles
     kb_finalize<<<n, b->max_ntiles <= 256 ? b->tune_final : kFinalThreads, 0,
                   s>>>(sl, work, b->bc);
+    // the per-filter spines on 256 threads while every slot has at most 256
+    // tiles (each thread then holds at most one tile, so the sums are those
+    // of 1024 threads): four times the spine CTAs fit on an SM
+    const int spt = b->max_ntiles <= 256 ? 256 : kSpineThreads;
     int launches = 2;
     if (WeightsFromLog<Real>::kExactNorm) {
         // the weights' sequential sum, whose reciprocal normalises them
         kb_exact_tiles<Real, false, true><<<nt, kThreads, 0, s>>>(sl, map);
-        kb_exact_spine<Real, false, true><<<n, kSpineThreads, 0, s>>>(sl,
+        kb_exact_spine<Real, false, true><<<n, spt, 0, s>>>(sl,
                                                                      work);
         launches += 2;
     }
     if (residual) {
         kb_tile_sums<Real, true><<<nt, kThreads, 0, s>>>(sl, map);
         if (sys)
-            kb_spine_weights<true, true><<<n, kSpineThreads, 0, s>>>(sl,
+            kb_spine_weights<true, true><<<n, spt, 0, s>>>(sl,
                                                                     work);
         else
-            kb_spine_weights<true, false><<<n, kSpineThreads, 0, s>>>(sl,
+            kb_spine_weights<true, false><<<n, spt, 0, s>>>(sl,
                                                                      work);
         launches += 2;
     }
@@ -1026,24 +1030,24 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
         launches += 1;
     } else if (!sys) {
         kb_sorted_tile_sums<<<nt, kThreads, 0, s>>>(sl, map);
-        kb_sorted_spine<<<n, kSpineThreads, 0, s>>>(sl, work);
+        kb_sorted_spine<<<n, spt, 0, s>>>(sl, work);
         kb_exact_terms_tiles<<<nt, kThreads, 0, s>>>(sl, map);
-        kb_exact_terms_spine<<<n, kSpineThreads, 0, s>>>(sl, work);
+        kb_exact_terms_spine<<<n, spt, 0, s>>>(sl, work);
         kb_sorted_uniforms<<<nt, kThreads, 0, s>>>(sl, map);
         launches += 5;
     }
     if (residual) {
         if (!WeightsFromLog<Real>::kApprox) { // the residuals' exact sum
             kb_exact_tiles<Real, true, true><<<nt, kThreads, 0, s>>>(sl, map);
-            kb_exact_spine<Real, true, true><<<n, kSpineThreads, 0, s>>>(
+            kb_exact_spine<Real, true, true><<<n, spt, 0, s>>>(
                 sl, work);
             launches += 2;
         }
         kb_exact_tiles<Real, true><<<nt, kThreads, 0, s>>>(sl, map);
-        kb_exact_spine<Real, true><<<n, kSpineThreads, 0, s>>>(sl, work);
+        kb_exact_spine<Real, true><<<n, spt, 0, s>>>(sl, work);
     } else {
         kb_exact_tiles<Real, false><<<nt, kThreads, 0, s>>>(sl, map);
-        kb_exact_spine<Real, false><<<n, kSpineThreads, 0, s>>>(sl, work);
+        kb_exact_spine<Real, false><<<n, spt, 0, s>>>(sl, work);
     }
     launches += 2;
     if (residual && sys)
@@ -1054,7 +1058,7 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
         kb_invert<Real, false, true><<<nt, kThreads, 0, s>>>(sl, map);
     else
         kb_invert<Real, false, false><<<nt, kThreads, 0, s>>>(sl, map);
-    kb_zero_spine<<<n, kSpineThreads, 0, s>>>(sl, work);
+    kb_zero_spine<<<n, spt, 0, s>>>(sl, work);
     kb_cfrp_fill<<<nt, kThreads, 0, s>>>(sl, map);
     kb_step_done<<<(n + 255) / 256, 256, 0, s>>>(b->d_slots, b->d_work, n);
     launches += 4;

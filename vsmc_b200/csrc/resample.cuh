@@ -2418,6 +2418,11 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
     // uniforms: up to the number of children (Nout when it is not N)
     const long long Nu = Nout > N ? Nout : N;
     const int ntu_dev = resample_ntiles(Nu);
+    // spines of at most 256 tiles on 256 threads: each thread holds at most
+    // one tile either way, so the sums are the same, with a quarter of the
+    // CTA to synchronise
+    const int spt = nt <= 256 ? 256 : kSpineThreads;
+    const int sptu = ntu_dev <= 256 ? 256 : kSpineThreads;
     const bool residual = scheme == VSMC_CUDA_RESIDUAL ||
                           scheme == VSMC_CUDA_RESIDUAL_STRATIFIED ||
                           scheme == VSMC_CUDA_RESIDUAL_SYSTEMATIC;
@@ -2434,17 +2439,17 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
             k_tile_sums<W, false><<<nt, kThreads, 0, s>>>(
                 wsrc, N, ws.ctl, ws.tile_sum, nullptr);
             if (sys)
-                k_spine_weights<false, true><<<1, kSpineThreads, 0, s>>>(
+                k_spine_weights<false, true><<<1, spt, 0, s>>>(
                     ws.tile_sum, nullptr, ws.tile_excl, nullptr, nt, N, eng,
                     ws.ctl);
             else
-                k_spine_weights<false, false><<<1, kSpineThreads, 0, s>>>(
+                k_spine_weights<false, false><<<1, spt, 0, s>>>(
                     ws.tile_sum, nullptr, ws.tile_excl, nullptr, nt, N, eng,
                     ws.ctl);
         }
         k_exact_tiles<W, false, true><<<exact_grid(nt), kThreads, 0, s>>>(
             wsrc, N, ws.ctl, ws.tile_excl, ws.ex);
-        k_exact_spine<W, false, true><<<1, kSpineThreads, 0, s>>>(
+        k_exact_spine<W, false, true><<<1, spt, 0, s>>>(
             wsrc, N, ws.ctl, nt, ws.ex);
         wx = with_exact_coeff(wsrc, &ws.ctl->coeff_w, ws.ex.rec);
     }
@@ -2452,22 +2457,22 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
         k_tile_sums<W, true><<<nt, kThreads, 0, s>>>(wx, N, ws.ctl,
                                                     ws.tile_sum, ws.tile_k);
         if (sys)
-            k_spine_weights<true, true><<<1, kSpineThreads, 0, s>>>(
+            k_spine_weights<true, true><<<1, spt, 0, s>>>(
                 ws.tile_sum, ws.tile_k, ws.tile_excl, ws.tile_kexcl, nt, N,
                 eng, ws.ctl);
         else
-            k_spine_weights<true, false><<<1, kSpineThreads, 0, s>>>(
+            k_spine_weights<true, false><<<1, spt, 0, s>>>(
                 ws.tile_sum, ws.tile_k, ws.tile_excl, ws.tile_kexcl, nt, N,
                 eng, ws.ctl);
     } else if (!spine_done && !W::kExactNorm) {
         k_tile_sums<W, false><<<nt, kThreads, 0, s>>>(wx, N, ws.ctl,
                                                      ws.tile_sum, nullptr);
         if (sys)
-            k_spine_weights<false, true><<<1, kSpineThreads, 0, s>>>(
+            k_spine_weights<false, true><<<1, spt, 0, s>>>(
                 ws.tile_sum, nullptr, ws.tile_excl, nullptr, nt, N, eng,
                 ws.ctl);
         else
-            k_spine_weights<false, false><<<1, kSpineThreads, 0, s>>>(
+            k_spine_weights<false, false><<<1, spt, 0, s>>>(
                 ws.tile_sum, nullptr, ws.tile_excl, nullptr, nt, N, eng,
                 ws.ctl);
     }
@@ -2491,13 +2496,13 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
     } else if (!sys && !sorted_ready) {
         k_sorted_tile_sums<<<ntu_dev, kThreads, 0, s>>>(eng, ws.ctl,
                                                         ws.u_tile_sum, ws.u);
-        k_sorted_spine<<<1, kSpineThreads, 0, s>>>(ws.u_tile_sum,
+        k_sorted_spine<<<1, sptu, 0, s>>>(ws.u_tile_sum,
                                                    ws.u_tile_excl, ws.ctl);
         // lmax exactly: the exact scan of the negated terms
         const TermsNeg tn{ws.u, 0};
         k_exact_tiles<TermsNeg, false><<<exact_grid(ntu_dev), kThreads, 0, s>>>(
             tn, Nu, ws.ctl, ws.u_tile_excl, ws.exu);
-        k_exact_spine<TermsNeg, false><<<1, kSpineThreads, 0, s>>>(
+        k_exact_spine<TermsNeg, false><<<1, sptu, 0, s>>>(
             tn, Nu, ws.ctl, ntu_dev, ws.exu);
         k_sorted_uniforms<<<ntu_dev, kThreads, 0, s>>>(ws.ctl, ws.exu, ws.u,
                                                        ws.bins);
@@ -2510,17 +2515,17 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
         if (!W::kApprox) {
             k_exact_tiles<W, true, true><<<exact_grid(nt), kThreads, 0, s>>>(
                 wx, N, ws.ctl, ws.tile_excl, ws.ex);
-            k_exact_spine<W, true, true><<<1, kSpineThreads, 0, s>>>(
+            k_exact_spine<W, true, true><<<1, spt, 0, s>>>(
                 wx, N, ws.ctl, nt, ws.ex);
         }
         k_exact_tiles<W, true><<<exact_grid(nt), kThreads, 0, s>>>(wx, N, ws.ctl,
                                                        ws.tile_excl, ws.ex);
-        k_exact_spine<W, true><<<1, kSpineThreads, 0, s>>>(wx, N, ws.ctl,
+        k_exact_spine<W, true><<<1, spt, 0, s>>>(wx, N, ws.ctl,
                                                            nt, ws.ex);
     } else {
         k_exact_tiles<W, false><<<exact_grid(nt), kThreads, 0, s>>>(wx, N, ws.ctl,
                                                         ws.tile_excl, ws.ex);
-        k_exact_spine<W, false><<<1, kSpineThreads, 0, s>>>(wx, N, ws.ctl,
+        k_exact_spine<W, false><<<1, spt, 0, s>>>(wx, N, ws.ctl,
                                                             nt, ws.ex);
     }
 #define VSMC_INVERT(R, S)                                                     \
@@ -2538,7 +2543,7 @@ inline void launch_resample_core(int scheme, W wsrc, long long N,
 #undef VSMC_INVERT
     if (cfrp) {
         // the spine kernel also advances the engine position
-        k_zero_spine<<<1, kSpineThreads, 0, s>>>(
+        k_zero_spine<<<1, spt, 0, s>>>(
             ws.tile_zeros, ws.tile_sinc_last, ws.zexcl, ws.tfirst, ws.tlast,
             nt, ws.ctl);
         k_cfrp_fill<<<nt, kThreads, 0, s>>>(N, ws.ctl, ws.sinc, ws.zexcl,
