@@ -241,18 +241,7 @@ kb_sorted_uniforms(const BatchSlot *slots, const TileRef *map)
 }
 
 // The exact lmax of a slot's sorted sequence (exact_scan.cuh over the
-// negated terms): per tile, then per slot.
-static __global__ void __launch_bounds__(kThreads, VSMC_EXACT_MIN_BLOCKS)
-kb_exact_terms_tiles(const BatchSlot *slots, const TileRef *map)
-{
-    __shared__ SmemExactTiles<false> sm;
-    const TileRef r = map[blockIdx.x];
-    const BatchSlot &b = slots[r.slot];
-    k_exact_tiles_body<TermsNeg, false>(TermsNeg{b.rws.u, 0}, b.N, b.rws.ctl,
-                                        b.rws.u_tile_excl, b.rws.exu, r.tile,
-                                        sm);
-}
-
+// negated terms): per slot (its tiles run in kb_exact_tiles_staged).
 static __global__ void __launch_bounds__(kSpineThreads)
 kb_exact_terms_spine(const BatchSlot *slots, const int32_t *work)
 {
@@ -276,17 +265,132 @@ kb_invert(const BatchSlot *slots, const TileRef *map)
         b.rws.tile_sinc_last, b.rws.ex, r.tile, sm);
 }
 
-// The exact cumulative weight (exact_scan.cuh): per tile, then per slot.
-template <typename Real, bool Residual, bool Raw = false>
-__global__ void __launch_bounds__(kThreads)
-kb_exact_tiles(const BatchSlot *slots, const TileRef *map)
+// The sources a batched exact scan runs over: a slot's weights (with the
+// normalisation pass's coefficient, or unnormalised for that pass) and its
+// sorted sequence's negated terms, with the approximate spine and the
+// ExactScan arrays that go with each.
+template <typename Real, bool Normed>
+struct SlotWeights {
+    typedef WeightsFromLog<Real> W;
+    __device__ static W get(const BatchSlot &b)
+    {
+        return batch_weights<Real>(b, Normed);
+    }
+    __device__ static const double *excl(const BatchSlot &b)
+    {
+        return b.rws.tile_excl;
+    }
+    __device__ static ExactScan scan(const BatchSlot &b) { return b.rws.ex; }
+};
+
+struct SlotTerms {
+    typedef TermsNeg W;
+    __device__ static W get(const BatchSlot &b) { return TermsNeg{b.rws.u, 0}; }
+    __device__ static const double *excl(const BatchSlot &b)
+    {
+        return b.rws.u_tile_excl;
+    }
+    __device__ static ExactScan scan(const BatchSlot &b) { return b.rws.exu; }
+};
+
+// Phase A of the exact scan over every (slot, tile) entry of the map: a
+// persistent grid whose CTAs stage the next entry's source values with
+// cp.async while they classify the current one (the single filter's
+// k_exact_tiles, over many filters).  Each entry computes what
+// k_exact_tiles_body computes for it, so the results are the same.
+template <typename Src, bool Residual, bool Raw>
+__global__ void __launch_bounds__(kThreads, VSMC_EXACT_STAGE_MIN_BLOCKS)
+kb_exact_tiles_staged(const BatchSlot *slots, const TileRef *map, int nmap)
 {
-    __shared__ SmemExactTiles<Residual> sm;
-    const TileRef r = map[blockIdx.x];
-    const BatchSlot &b = slots[r.slot];
-    k_exact_tiles_body<WeightsFromLog<Real>, Residual, Raw>(
-        batch_weights<Real>(b, Residual || !Raw), b.N, b.rws.ctl,
-        b.rws.tile_excl, b.rws.ex, r.tile, sm);
+    typedef typename Src::W W;
+    typedef typename W::stage_t S;
+    __shared__ SmemExactStage sm;
+    // the scanned length of an entry's slot, or -1 when the entry's tile
+    // is not scanned (no resampling, past the length, or residual children
+    // none: then only the integer parts are stored)
+    const auto length = [&](const BatchSlot &b, const W &w, int tile,
+                            bool &none) -> long long {
+        const ResampleCtl *ctl = b.rws.ctl;
+        none = false;
+        if (!w.active(ctl))
+            return -1;
+        const long long N = w.length(ctl, b.N);
+        if ((long long)tile * kTile >= N)
+            return -1;
+        none = Residual && ctl->NN <= 0;
+        if (none && Raw)
+            return -1;
+        return N;
+    };
+    const auto issue = [&](int m, int buf) {
+        const TileRef r = map[m];
+        const BatchSlot &b = slots[r.slot];
+        const W w = Src::get(b);
+        bool none;
+        const long long N = length(b, w, r.tile, none);
+        if (N > 0) {
+            S *dst = reinterpret_cast<S *>(sm.stage[buf]);
+            const S *src = w.stage_src();
+            const long long base = (long long)r.tile * kTile;
+#pragma unroll
+            for (int j = 0; j < kItems; ++j) {
+                const int l = j * kThreads + threadIdx.x;
+                if (base + l < N)
+                    cp_async_n<sizeof(S)>(&dst[pad8(l)], &src[base + l]);
+            }
+        }
+        cp_async_commit(); // (an empty group keeps the counting uniform)
+    };
+    int buf = 0;
+    if ((int)blockIdx.x < nmap)
+        issue(blockIdx.x, 0);
+    for (int m = blockIdx.x; m < nmap; m += gridDim.x) {
+        const int next = m + gridDim.x;
+        if (next < nmap) {
+            issue(next, buf ^ 1);
+            cp_async_wait_one();
+        } else {
+            cp_async_wait_all();
+        }
+        __syncthreads();
+        const TileRef r = map[m];
+        const BatchSlot &b = slots[r.slot];
+        W w = Src::get(b);
+        bool none;
+        const long long N = length(b, w, r.tile, none);
+        if (N > 0) {
+            const ResampleCtl *ctl = b.rws.ctl;
+            const ExactScan ex = Src::scan(b);
+            w.prepare();
+            const double Nd = (double)resample_children(ctl, N);
+            const double coeff_r = Residual && !Raw ? ctl->coeff_r : 1.0;
+            const S *st = reinterpret_cast<const S *>(sm.stage[buf]);
+            const long long i0 =
+                (long long)r.tile * kTile + (long long)threadIdx.x * kItems;
+            double wv[kItems];
+            int32_t kk[kItems];
+#pragma unroll
+            for (int j = 0; j < kItems; ++j) {
+                double k = 0.0;
+                wv[j] = i0 + j < N
+                            ? scan_weight_staged<W, Residual, Raw>(
+                                  w, st[pad8(threadIdx.x * kItems + j)], Nd,
+                                  coeff_r, k)
+                            : 0.0;
+                kk[j] = (int32_t)k;
+            }
+            if (none) {
+                if (i0 < N)
+                    store8(ex.kint, i0, N, kk);
+            } else {
+                exact_tile_compute<W, Residual, Raw>(w, N, ctl, Src::excl(b),
+                                                     ex, r.tile, coeff_r, wv,
+                                                     kk, sm.core);
+            }
+        }
+        __syncthreads(); // every read of stage[buf] before it is refilled
+        buf ^= 1;
+    }
 }
 
 template <typename Real, bool Residual, bool Raw = false>
@@ -1010,7 +1114,8 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
     int launches = 2;
     if (WeightsFromLog<Real>::kExactNorm) {
         // the weights' sequential sum, whose reciprocal normalises them
-        kb_exact_tiles<Real, false, true><<<nt, kThreads, 0, s>>>(sl, map);
+        kb_exact_tiles_staged<SlotWeights<Real, false>, false, true>
+            <<<exact_grid((int)nt), kThreads, 0, s>>>(sl, map, (int)nt);
         kb_exact_spine<Real, false, true><<<n, spt, 0, s>>>(sl,
                                                                      work);
         launches += 2;
@@ -1031,22 +1136,26 @@ void launch_batch_step(vsmc_cuda_cv_batch *b, int n, long long tiles,
     } else if (!sys) {
         kb_sorted_tile_sums<<<nt, kThreads, 0, s>>>(sl, map);
         kb_sorted_spine<<<n, spt, 0, s>>>(sl, work);
-        kb_exact_terms_tiles<<<nt, kThreads, 0, s>>>(sl, map);
+        kb_exact_tiles_staged<SlotTerms, false, false>
+            <<<exact_grid((int)nt), kThreads, 0, s>>>(sl, map, (int)nt);
         kb_exact_terms_spine<<<n, spt, 0, s>>>(sl, work);
         kb_sorted_uniforms<<<nt, kThreads, 0, s>>>(sl, map);
         launches += 5;
     }
     if (residual) {
         if (!WeightsFromLog<Real>::kApprox) { // the residuals' exact sum
-            kb_exact_tiles<Real, true, true><<<nt, kThreads, 0, s>>>(sl, map);
+            kb_exact_tiles_staged<SlotWeights<Real, true>, true, true>
+                <<<exact_grid((int)nt), kThreads, 0, s>>>(sl, map, (int)nt);
             kb_exact_spine<Real, true, true><<<n, spt, 0, s>>>(
                 sl, work);
             launches += 2;
         }
-        kb_exact_tiles<Real, true><<<nt, kThreads, 0, s>>>(sl, map);
+        kb_exact_tiles_staged<SlotWeights<Real, true>, true, false>
+            <<<exact_grid((int)nt), kThreads, 0, s>>>(sl, map, (int)nt);
         kb_exact_spine<Real, true><<<n, spt, 0, s>>>(sl, work);
     } else {
-        kb_exact_tiles<Real, false><<<nt, kThreads, 0, s>>>(sl, map);
+        kb_exact_tiles_staged<SlotWeights<Real, true>, false, false>
+            <<<exact_grid((int)nt), kThreads, 0, s>>>(sl, map, (int)nt);
         kb_exact_spine<Real, false><<<n, spt, 0, s>>>(sl, work);
     }
     launches += 2;
