@@ -154,6 +154,18 @@ __device__ __forceinline__ double canonical_u32x2(uint32_t a, uint32_t b)
     return r >= 1.0 ? 0x1.fffffffffffffp-1 : r;
 }
 
+// 2U - 1 of the canonical double U above, in one rounding: with d the
+// rounded 64-bit integer, 2U = d * 2^-63 is exact, so fma(d, 2^-63, -1)
+// rounds d * 2^-63 - 1 once, exactly as 2U - 1 does.  When d rounds up to
+// 2^64, U is clamped to 1 - 2^-53 and 2U - 1 is 1 - 2^-52; the fma gives 1.0
+// there and is clamped to the same value.
+__device__ __forceinline__ double polar_coord_u32x2(uint32_t a, uint32_t b)
+{
+    const unsigned long long x = ((unsigned long long)b << 32) | a;
+    const double r = __fma_rn(__ull2double_rn(x), 0x1p-63, -1.0);
+    return r >= 1.0 ? 0x1.ffffffffffffep-1 : r;
+}
+
 // ------------------------------------------------------ polar normals ------
 // A Philox4x32 stream positioned at a block boundary: every polar attempt of
 // libstdc++'s normal_distribution consumes exactly four 32-bit words (two
@@ -183,8 +195,8 @@ __device__ __forceinline__ void polar_accept(PhiloxStream &s, double &x,
 {
     do {
         const uint4 w = s.next_block();
-        x = __dadd_rn(__dmul_rn(2.0, canonical_u32x2(w.x, w.y)), -1.0);
-        y = __dadd_rn(__dmul_rn(2.0, canonical_u32x2(w.z, w.w)), -1.0);
+        x = polar_coord_u32x2(w.x, w.y);
+        y = polar_coord_u32x2(w.z, w.w);
         r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
     } while (r2 > 1.0 || r2 == 0.0);
 }
@@ -193,8 +205,8 @@ __device__ __forceinline__ void polar_accept(PhiloxStream &s, double &x,
 __device__ __forceinline__ void polar_point(const uint4 &w, double &x,
                                             double &y, double &r2)
 {
-    x = __dadd_rn(__dmul_rn(2.0, canonical_u32x2(w.x, w.y)), -1.0);
-    y = __dadd_rn(__dmul_rn(2.0, canonical_u32x2(w.z, w.w)), -1.0);
+    x = polar_coord_u32x2(w.x, w.y);
+    y = polar_coord_u32x2(w.z, w.w);
     r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
 }
 
