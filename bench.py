@@ -218,6 +218,50 @@ def forms_compare(capi, N, sch, K, W, ox, oy, sp, fp64_step_ms):
                             "copy_from vectors (fixed ancestry) over the same T steps"}
 
 
+def mixed_error_sample(capi, cases, scheme=0):
+    """The mixed form's error against FP64 for a sample of filters, on a
+    fixed ancestry: for each (N, T, ox, oy, seed, stream_id) the FP64 filter
+    records its resampling decisions and copy_from vectors and the mixed
+    filter replays them.  Batched filters and served requests give the same
+    results as the same filter run alone (bit for bit in both forms), so
+    this is the error of their results."""
+    import numpy as np
+    import torch
+
+    errs, rows = [], []
+    for (N, T, ox, oy, seed, sid) in cases:
+        rec = torch.empty(T * N, dtype=torch.int32, device="cuda")
+        with capi.CVFilter(N, T, scheme=scheme, form=capi.FP64, seed=seed,
+                           stream_id=sid) as f:
+            f.set_observations_host(ox, oy)
+            f.set_ancestry(record_ptr=rec.data_ptr())
+            f.initialize()
+            f.iterate(T - 1)
+            h64 = f.history()
+            z64 = f.log_evidence()
+        flags = torch.from_numpy(h64["resampled"].astype("int32")).cuda()
+        with capi.CVFilter(N, T, scheme=scheme, form=capi.MIXED, seed=seed,
+                           stream_id=sid) as m:
+            m.set_observations_host(ox, oy)
+            m.set_ancestry(replay_ptr=rec.data_ptr(),
+                           replay_flags_ptr=flags.data_ptr())
+            m.initialize()
+            m.iterate(T - 1)
+            z32 = m.log_evidence()
+        del rec
+        errs.append(abs(z32 - z64) / abs(z64))
+        rows.append({"N": int(N), "T": int(T), "log_evidence_fp64": float(z64),
+                     "abs_error": float(abs(z32 - z64))})
+    torch.cuda.synchronize()
+    worst = int(np.argmax(errs))
+    return {"filters": len(errs), "max_rel_log_evidence_error": float(np.max(errs)),
+            "median_rel_log_evidence_error": float(np.median(errs)),
+            "max_abs_log_evidence_error": float(max(r["abs_error"] for r in rows)),
+            "worst": rows[worst],
+            "method": "fixed ancestry: the mixed run replays the FP64 run's resampling "
+                      "decisions and copy_from vectors"}
+
+
 def scheme_sweep(capi, sp, sizes=(1 << 16, 1 << 20, 1 << 24), K=20, W=3,
                  cpu=True):
     """Every resampling scheme at N = 2^16, 2^20, 2^24 in both forms: device
@@ -310,6 +354,20 @@ def batched_run(capi, form, N, T, obs, reps=3, autotune=True):
             "launch_shape": {"move_ctas_per_sm": shape[0], "finalize_threads": shape[1]}}
 
 
+def serving_requests(lam, seed, max_requests=2000):
+    """The request arrivals of one serving point: their number, arrival
+    times over min(1 s, max_requests / lam) and sizes N (log-uniform on
+    [2^10, 2^18])."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    window = min(1.0, max_requests / lam)
+    n = max(1, min(max_requests, int(rng.poisson(lam * window))))
+    arr = np.sort(rng.uniform(0.0, window, n))
+    Ns = np.exp(rng.uniform(np.log(2 ** 10), np.log(2 ** 18), n)).astype(np.int64)
+    return n, arr, Ns
+
+
 def serving_point(capi, form, lam, seed, T=100, period_s=1e-3, max_requests=2000,
                   budget=16 << 30):
     """Poisson request arrivals at rate `lam`; request N log-uniform on
@@ -319,11 +377,7 @@ def serving_point(capi, form, lam, seed, T=100, period_s=1e-3, max_requests=2000
     max_requests / lam)."""
     import numpy as np
 
-    rng = np.random.default_rng(seed)
-    window = min(1.0, max_requests / lam)
-    n = max(1, min(max_requests, int(rng.poisson(lam * window))))
-    arr = np.sort(rng.uniform(0.0, window, n))
-    Ns = np.exp(rng.uniform(np.log(2 ** 10), np.log(2 ** 18), n)).astype(np.int64)
+    n, arr, Ns = serving_requests(lam, seed, max_requests)
     obs = [capi.cv_simulate(T, obs_seed=5000 + k, stream_id=k) for k in range(n)]
     ox = np.stack([o[0] for o in obs])
     oy = np.stack([o[1] for o in obs])
@@ -665,6 +719,10 @@ def main():
             "mixed": batched_run(capi, capi.MIXED, bN, bT, bobs)}
         b64, b32 = extras["batched"]["fp64"], extras["batched"]["mixed"]
         extras["batched"]["speedup_mixed_vs_fp64"] = b32["filters_per_s"] / b64["filters_per_s"]
+        # every 256th filter of the batch (16 filters)
+        b32["error_vs_fp64"] = mixed_error_sample(
+            capi, [(int(bN[k]), int(bT[k]), bobs[k][0], bobs[k][1], 101 + k, k)
+                   for k in range(0, len(bN), 256)])
         gdata = capi.gmm_simulate(1000, 1)
         g64 = gmm_run(capi, capi.FP64, gdata)
         g32 = gmm_run(capi, capi.MIXED, gdata)
@@ -686,6 +744,12 @@ def main():
                         "HBM budget 16 GiB; latency = result on host - arrival",
             "fp64": [serving_point(capi, capi.FP64, lam, 11) for lam in rates],
             "mixed": [serving_point(capi, capi.MIXED, lam, 11) for lam in rates]}
+        # the first 16 requests of the busiest point
+        _, _, sNs = serving_requests(max(rates), 11)
+        extras["serving"]["mixed_error_vs_fp64"] = mixed_error_sample(
+            capi, [(int(sNs[k]), 100) + tuple(capi.cv_simulate(100, obs_seed=5000 + k,
+                                                               stream_id=k)) + (101 + k, k)
+                   for k in range(min(16, len(sNs)))])
 
     cpu = None
     # the host reference runs the filter at threshold 0.5
