@@ -15,28 +15,38 @@
 
 namespace vsmc_b200 {
 
+// Philox blocks a particle draws up front for its two polar points.  Four
+// measured best at 2^24 particles (the FP64 move 0.692 ms with three, 0.684
+// with four, 0.70 with five and 0.73 with six, which spill).
+#ifndef VSMC_POLAR_UPFRONT
+#define VSMC_POLAR_UPFRONT 4
+#endif
+
 // The first two accepted polar points of a particle stream (libstdc++'s
-// two calls of the polar loop).  Three blocks are drawn up front: their
-// Philox chains are independent, so they overlap in the pipeline, and 88%
-// of particles need no more; the rest continue one block at a time.  The
-// points are exactly those of the sequential loop, in stream order.
+// two calls of the polar loop).  VSMC_POLAR_UPFRONT blocks are drawn up
+// front: their Philox chains are independent, so they overlap in the
+// pipeline, and with four 97% of particles need no more (88% with three,
+// and a warp with any such lane runs the extra block anyway); the rest
+// continue one block at a time.  The points are exactly those of the
+// sequential loop, in stream order.
 __device__ __forceinline__ void polar_two(uint32_t iter, uint32_t id,
                                           uint32_t stream, uint32_t k0,
                                           uint32_t k1, double &x1, double &y1,
                                           double &q1, double &x2, double &y2,
                                           double &q2)
 {
-    uint4 w[3];
-    double x[3], y[3], r[3];
+    constexpr int U = VSMC_POLAR_UPFRONT;
+    uint4 w[U];
+    double x[U], y[U], r[U];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < U; ++k) {
         w[k] = philox4x32_10(make_uint4((uint32_t)(k + 1), iter, id, stream),
                              k0, k1);
         polar_point(w[k], x[k], y[k], r[k]);
     }
     int n = 0;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < U; ++k) {
         if (polar_ok(r[k])) {
             if (n == 0) {
                 x1 = x[k];
@@ -52,7 +62,7 @@ __device__ __forceinline__ void polar_two(uint32_t iter, uint32_t id,
     }
     if (n < 2) {
         PhiloxStream s;
-        s.ctr = make_uint4(3u, iter, id, stream);
+        s.ctr = make_uint4((uint32_t)U, iter, id, stream);
         s.k0 = k0;
         s.k1 = k1;
         double a, b, c;
